@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Benchmark of the first-order finite-volume step (the reference's `launcher` path).
+
+Workload at N=1: the 2D blast on a 40000 x 20000 grid in FP64 through the plain path,
+one step = one launcher call over the whole grid followed by the host Dt read-back of
+the reference loop (hydro2d/main.cxx:734-747). Inputs (51.2 GB double-buffered) are far
+larger than L2, so no flush is needed between steps.
+
+  value      whole-job cell-updates/s with the state resident in HBM (CUDA events)
+  e2e        the same metric through the C-ABI drop-in `launcher` with the reference
+             host loop's per-step traffic: ghost rows host->device from pinned memory,
+             launcher, Dt and edge rows device->host (hydro2d/main.cxx:720-763)
+  roofline   the strip kernel's algorithmic bytes (64 B per FP64 2D cell-update, the
+             reference's own byte model, hydro2d/main.cxx:889) over its event-timed
+             duration, against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own kernel.cxx (oracle/_ref) on the host cores, on a
+             bounded sample of the same workload (rank 0, N=1)
+  variants   FP32 2D and FP64/FP32 3D 512^3 plain-path numbers (a few steps each)
+
+`--impl reference` times the reference's CPU kernel alone on the same metric.
+Under torchrun (N>1) each rank runs its own replica (no data-path collective; weak
+scaling) and rank 0 prints the max-over-ranks timing.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from datetime import timedelta
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "scalable-fpga-hydrodynamics_b200"
+METRIC = "GCell-upd/s batched FP32 vs plain FP64 @<=1e-5 rel err; p50/p99 latency"
+UNIT = "GCell-upd/s"
+BYTES_PER_CELL = {(2, 8): 64, (2, 4): 32, (3, 8): 80, (3, 4): 40}
+
+
+def load_pkg():
+    name = "hydro_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, PKG / "__init__.py", submodule_search_locations=[str(PKG)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------- clocks ---
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# -------------------------------------------------------------- GPU measurements ---
+def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0):
+    """Host loop with the state resident on the device; CUDA events on the launching
+    stream: total time of `steps` steps and per-step kernel time."""
+    run = hb.BlastRun(nb, T, kernel=kernel)
+    for _ in range(warmup):
+        run.step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    E = torch.cuda.Event
+    e_start, e_end = E(enable_timing=True), E(enable_timing=True)
+    per = [(E(enable_timing=True), E(enable_timing=True)) for _ in range(steps)]
+    e_start.record(stream)
+    for k in range(steps):
+        per[k][0].record(stream)
+        run.step_kernel_only()
+        per[k][1].record(stream)
+        run.step_finish()
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    total_ms = e_start.elapsed_time(e_end)
+    kern_ms = [a.elapsed_time(b) for a, b in per]
+    info = run.last_info
+    res = dict(total_ms=total_ms, kernel_ms=kern_ms, kernel=int(info.kernel), it=run.it)
+    del run
+    torch.cuda.empty_cache()
+    return res
+
+
+def bench_e2e(hb, torch, nb, T, steps, warmup):
+    """The reference host loop through the drop-in launcher (C ABI): per step, ghost
+    rows host->device from pinned memory, launcher, Dt and edge rows device->host."""
+    phys = hb.Physics(T, nb)
+    tdt = torch.float64 if T is np.float64 else torch.float32
+    cur = hb.alloc_state(nb, T)
+    nxt = hb.alloc_state(nb, T)
+    dt_dev = torch.zeros(1, dtype=tdt, device="cuda")
+    dt = hb.init_blast(cur, phys)
+    ys = nb[1] + 2
+    row = 2 * ys  # elements per row per array
+    # host copies of the rows the reference host keeps current: ghost 0, 1, nb_x, ghost nb_x+1
+    h_rows = torch.zeros((2, 4, row), dtype=tdt, pin_memory=True)
+    h_dt = torch.zeros(1, dtype=tdt, pin_memory=True)
+    for a in range(2):
+        h_rows[a, 1].copy_(cur[a][row * 1:row * 2])
+        h_rows[a, 2].copy_(cur[a][row * nb[0]:row * (nb[0] + 1)])
+    stream = torch.cuda.current_stream()
+    big = T(1e20)
+
+    def one_step(cur, nxt, dt):
+        # host ghost exchange (hydro2d/main.cxx:349-378) then H2D of the ghost rows
+        for a in range(2):
+            h_rows[a, 0].copy_(h_rows[a, 2])
+            h_rows[a, 3].copy_(h_rows[a, 1])
+            cur[a][0:row].copy_(h_rows[a, 0], non_blocking=True)
+            cur[a][row * (nb[0] + 1):row * (nb[0] + 2)].copy_(h_rows[a, 3], non_blocking=True)
+        dtd = phys.dtd(dt)
+        us = hb.launcher2d(cur[0], cur[1], nxt[0], nxt[1], dt_dev, phys.C_min, phys.g, phys.gm1, phys.divgamma,
+                           phys.k, nb[0], nb[1], dtd[0], dtd[1])
+        if us < 0:
+            raise RuntimeError(hb.last_error())
+        h_dt.copy_(dt_dev, non_blocking=True)
+        for a in range(2):
+            h_rows[a, 1].copy_(nxt[a][row * 1:row * 2], non_blocking=True)
+            h_rows[a, 2].copy_(nxt[a][row * nb[0]:row * (nb[0] + 1)], non_blocking=True)
+        stream.synchronize()
+        dtn = T(h_dt.item())
+        return nxt, cur, (dtn if dtn < big else big)
+
+    for _ in range(warmup):
+        cur, nxt, dt = one_step(cur, nxt, dt)
+    torch.cuda.synchronize()
+    E = torch.cuda.Event
+    e0, e1 = E(enable_timing=True), E(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(steps):
+        cur, nxt, dt = one_step(cur, nxt, dt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    ev_ms = e0.elapsed_time(e1)
+    isz = 8 if T is np.float64 else 4
+    h2d = 2 * 2 * row * isz
+    d2h = isz + 2 * 2 * row * isz
+    del cur, nxt
+    torch.cuda.empty_cache()
+    return dict(ms=max(wall_ms, ev_ms), h2d=h2d, d2h=d2h)
+
+
+# -------------------------------------------------------------- CPU (reference) ---
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def has_avx2_fma():
+    try:
+        flags = Path("/proc/cpuinfo").read_text()
+        return " avx2" in flags and " fma" in flags
+    except Exception:
+        return False
+
+
+def cpu_reference_sample(nb_y: int, rows: int, seconds: float, threads: int):
+    """The reference's own kernel.cxx (oracle/_ref, FMA-contracting build as in the
+    reference Makefile) on `threads` host threads, each stepping its own rows x nb_y
+    slab of the blast (the reference's X-slab decomposition, one slab per core) for
+    about `seconds`. Falls back to the oracle restatement when oracle/_ref is absent.
+    Returns (cell-updates/s, kind, description)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+
+    hb = load_pkg()
+    T = np.float64
+    nb = (rows, nb_y)
+    phys = hb.Physics(T, (40000, nb_y))  # the full workload's constants
+    phys.nb = nb
+    o = orc.Oracle()
+    kind = "reference"
+    if orc.available_ref(2, T, fast=True) and has_avx2_fma():
+        stepper = orc.RefKernel(2, T, fast=True).step
+        what = "oracle/_ref/libref2d_f64_fast.so (reference kernel.cxx, -O2 -march=x86-64-v3)"
+    elif orc.available_ref(2, T):
+        stepper = orc.RefKernel(2, T).step
+        what = "oracle/_ref/libref2d_f64.so (reference kernel.cxx, -O2 -ffp-contract=off)"
+    else:
+        stepper = o.step
+        kind = "port"
+        what = "oracle/liboracle.so (C restatement)"
+    threading.stack_size(64 << 20)  # the reference kernel keeps a 2 MB line buffer on the stack
+    dtd = phys.dtd(T(5e-6))
+    counts = [0] * threads
+    stop = threading.Event()
+
+    def work(tid):
+        ncell = (rows + 2) * (nb_y + 2)
+        a = (np.zeros(2 * ncell, T), np.zeros(2 * ncell, T))
+        b = (np.zeros(2 * ncell, T), np.zeros(2 * ncell, T))
+        o.init(a, phys)
+        stepper(a, b, phys, dtd)  # warm-up
+        while not stop.is_set():
+            orc.ghost_x_numpy(a, nb)
+            stepper(a, b, phys, dtd)
+            a, b = b, a
+            counts[tid] += 1
+
+    ths = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+    for th in ths:
+        th.start()
+    time.sleep(0.5)
+    c0 = sum(counts)
+    t0 = time.perf_counter()
+    time.sleep(seconds)
+    c1 = sum(counts)
+    t1 = time.perf_counter()
+    stop.set()
+    for th in ths:
+        th.join()
+    cells = (c1 - c0) * rows * nb_y
+    return cells / (t1 - t0), kind, what
+
+
+# ------------------------------------------------------------------------ main ---
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nb", type=int, nargs=2, default=[40000, 20000])
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    assert args.warmup >= 3 or args.nb != [40000, 20000], "at least 3 warm-up steps"
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nb = tuple(args.nb)
+    workload = f"2D blast {nb[0]}x{nb[1]} FP64, plain path (one launcher call per step)"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        thr = cpu_threads()
+        rows = 32
+        per_step = []
+        for k in range(args.warmup + args.steps):
+            rate, kind, what = cpu_reference_sample(nb[1], rows, 2.0 if k >= args.warmup else 0.5, thr)
+            if k >= args.warmup:
+                per_step.append(rate)
+        rate = statistics.median(per_step)
+        v = rate / 1e9
+        sample = f"{thr} threads x {rows}x{nb[1]} slabs of the blast, ~2 s per step ({what})"
+        line = dict(metric=METRIC, value=v, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=nb[0] * nb[1] / rate * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None,
+                    dtype="f64", data="synthetic (reference blast IC)", impl="reference",
+                    config=dict(workload=workload, nb_x=nb[0], nb_y=nb[1], l2="inputs larger than L2"),
+                    cpu_baseline=dict(value=v, unit=UNIT, cores=thr, kind=kind, sample=sample),
+                    e2e=dict(value=v, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    hb = load_pkg()
+    hb.build()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    hbm, peak_kind = peaks()
+    cells = nb[0] * nb[1]
+
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    r = bench_resident(hb, torch, nb, np.float64, args.steps, args.warmup)
+    clocks = sampler.stop()
+    barrier()
+    total_ms = max_over_ranks(r["total_ms"])
+    ms_step = total_ms / args.steps
+    value = world * cells * args.steps / (total_ms / 1e3) / 1e9
+    kern_ms = statistics.mean(r["kernel_ms"])
+    achieved = cells * BYTES_PER_CELL[(2, 8)] / (kern_ms / 1e3) / 1e9
+    roofline = dict(bound="hbm", achieved=achieved, peak=hbm, unit="GB/s", frac=achieved / hbm,
+                    peak_kind=peak_kind, traffic=None, kernel="strip2d<double>",
+                    bytes_per_cell=BYTES_PER_CELL[(2, 8)], kernel_ms=kern_ms)
+    tp = ROOT / "profiles" / "traffic.json"
+    if tp.exists():
+        tr = json.loads(tp.read_text()).get("strip2d_f64_bytes_per_cell")
+        if tr:
+            roofline["traffic"] = tr * cells
+
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        e = bench_e2e(hb, torch, nb, np.float64, max(3, args.steps // 3), 2)
+        barrier()
+        e_ms = max_over_ranks(e["ms"])
+        nst = max(3, args.steps // 3)
+        e2e = dict(value=world * cells * nst / (e_ms / 1e3) / 1e9, unit=UNIT, h2d_bytes_per_step=e["h2d"],
+                   d2h_bytes_per_step=e["d2h"], path="drop-in launcher (C ABI) + reference host-loop copies")
+
+    variants = {}
+    if not args.no_variants:
+        for name, vnb, T in (("2d_f32_40000x20000", nb, np.float32), ("3d_f64_512^3", (512, 512, 512), np.float64),
+                             ("3d_f32_512^3", (512, 512, 512), np.float32)):
+            barrier()
+            vr = bench_resident(hb, torch, vnb, T, max(5, args.steps // 3), 3)
+            barrier()
+            vms = max_over_ranks(vr["total_ms"])
+            nst = max(5, args.steps // 3)
+            vc = int(np.prod(vnb))
+            km = statistics.mean(vr["kernel_ms"])
+            bpc = BYTES_PER_CELL[(len(vnb), np.dtype(T).itemsize)]
+            variants[name] = dict(value=world * vc * nst / (vms / 1e3) / 1e9, unit=UNIT,
+                                  kernel_gbs=vc * bpc / (km / 1e3) / 1e9, frac=vc * bpc / (km / 1e3) / 1e9 / hbm,
+                                  kernel=int(vr["kernel"]), ms_per_step=vms / nst)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        thr = cpu_threads()
+        rate, kind, what = cpu_reference_sample(nb[1], 32, 3.0, thr)
+        cpu = dict(value=rate / 1e9, unit=UNIT, cores=thr, kind=kind,
+                   sample=f"{thr} threads x 32x{nb[1]} slabs of the blast for 3 s ({what})")
+
+    if rank == 0:
+        line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=ms_step, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+                    data="synthetic (reference blast IC, built on the device)",
+                    config=dict(workload=workload, nb_x=nb[0], nb_y=nb[1], l2="inputs larger than L2 (51.2 GB)",
+                                parallelism=f"replicas x{world}"),
+                    roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps, clocks=clocks,
+                    variants=variants)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,155 @@
+/*
+ * C ABI of the B200 finite-volume library (libhydro_b200.so).
+ *
+ * The reference exposes one device entry point per program, the C-linkage
+ *   extern "C" double launcher(...)
+ * declared in hydro2d/kernel.hpp:63-68 (2D) and hydro3d/kernel.hpp:64-69 (3D), once
+ * per precision (DATATYPE = double, or float under USE_FLOAT, kernel.hpp:9-39).
+ * Because all four share the symbol name `launcher`, this library exports them under
+ * distinct names; four thin drop-in libraries re-export each one as `launcher`:
+ *
+ *   libhydro2d.so        launcher == hydro2d_launcher_f64
+ *   libhydro2d_float.so  launcher == hydro2d_launcher_f32
+ *   libhydro3d.so        launcher == hydro3d_launcher_f64
+ *   libhydro3d_float.so  launcher == hydro3d_launcher_f32
+ *
+ * Conventions shared by every launcher (the reference's, hydro2d/kernel.cxx:331-367):
+ *  - device pointers are owned by the caller (hydro2d/main.cxx:125-129);
+ *  - NB_X/NB_Y[/NB_Z] are interior sizes, arrays hold NB+2 cells per axis;
+ *  - DtDx/DtDy[/DtDz] arrive by const reference in the reference, i.e. as pointers to
+ *    host memory at the ABI; they are read on the host before the launch;
+ *  - the call is synchronous and returns the elapsed microseconds measured on the host
+ *    around launch and completion (feeds T->total_compute, hydro2d/main.cxx:767);
+ *  - on a CUDA or argument error it returns a negative value, prints one line to
+ *    stderr and latches the error for hydro_last_error(); it never aborts;
+ *  - X is periodic by in-kernel wrap over the whole domain: the ghost rows/planes of
+ *    the input are not read, so the host's ghost copies (hydro2d/main.cxx:720-729) are
+ *    harmless but unnecessary; Y (and Z) walls are reflective.
+ *  - the sycl::queue by-value argument becomes hydro_queue_t, a trivially copyable
+ *    struct holding the CUDA stream; include/compat/sycl/sycl.hpp defines sycl::queue
+ *    with exactly this layout so an unchanged main.cxx calls these entry points.
+ */
+#ifndef HYDRO_B200_H
+#define HYDRO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The queue a launcher runs on: a CUDA stream (NULL = legacy default stream) and the
+ * device it belongs to (-1 = the current device). */
+typedef struct hydro_queue {
+    void *stream;
+    int device;
+    int flags;
+} hydro_queue_t;
+
+/* Extra results of one step, beyond what the reference's launcher returns. */
+typedef struct hydro_step_info {
+    double mass;      /* compensated FP64 sum of the new interior density */
+    double max_speed; /* max over interior cells of c_s + |u| (Dt_next = C_min / this) */
+    unsigned err;     /* bit 0: non-physical state; bit 1: a bounded wait timed out */
+    int kernel;       /* 1 = TMA strip kernel, 2 = direct kernel */
+} hydro_step_info_t;
+
+/* Kernel selection for the *_step entry points */
+#define HYDRO_KERNEL_AUTO 0
+#define HYDRO_KERNEL_STRIP 1
+#define HYDRO_KERNEL_DIRECT 2
+
+/* Return codes */
+#define HYDRO_OK 0
+#define HYDRO_ERR_ARG (-1)
+#define HYDRO_ERR_CUDA (-2)
+#define HYDRO_ERR_NONPHYSICAL (-3)
+#define HYDRO_ERR_TIMEOUT (-4)
+
+/* ---- drop-in launchers ---------------------------------------------------------- */
+
+/* Replaces `launcher` of hydro2d/kernel.hpp:63-68 with DATATYPE = double. */
+double hydro2d_launcher_f64(const double *d_rhoE, const double *d_uv, double *d_rhoE_next, double *d_uv_next,
+                            double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma,
+                            double K, size_t NB_X, size_t NB_Y, const double *DtDx, const double *DtDy,
+                            hydro_queue_t queue);
+
+/* Replaces `launcher` of hydro2d/kernel.hpp:63-68 with DATATYPE = float (USE_FLOAT). */
+double hydro2d_launcher_f32(const float *d_rhoE, const float *d_uv, float *d_rhoE_next, float *d_uv_next,
+                            float *Dt_next, float C_min, float gamma, float gamma_minus_one, float divgamma, float K,
+                            size_t NB_X, size_t NB_Y, const float *DtDx, const float *DtDy, hydro_queue_t queue);
+
+/* Replaces `launcher` of hydro3d/kernel.hpp:64-69 with DATATYPE = double. */
+double hydro3d_launcher_f64(const double *d_rhoE, const double *d_uvw, double *d_rhoE_next, double *d_uvw_next,
+                            double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma,
+                            double K, size_t NB_X, size_t NB_Y, size_t NB_Z, const double *DtDx, const double *DtDy,
+                            const double *DtDz, hydro_queue_t queue);
+
+/* Replaces `launcher` of hydro3d/kernel.hpp:64-69 with DATATYPE = float (USE_FLOAT). */
+double hydro3d_launcher_f32(const float *d_rhoE, const float *d_uvw, float *d_rhoE_next, float *d_uvw_next,
+                            float *Dt_next, float C_min, float gamma, float gamma_minus_one, float divgamma, float K,
+                            size_t NB_X, size_t NB_Y, size_t NB_Z, const float *DtDx, const float *DtDy,
+                            const float *DtDz, hydro_queue_t queue);
+
+/* ---- step entry points with explicit stream, kernel choice and results ------------ */
+/* Same arithmetic as the launchers (hydro2d/kernel.cxx:132-319, hydro3d/kernel.cxx:
+ * 145-407) with DtDx.. by value. sync = 0 only enqueues on `stream` (info->kernel is
+ * still set); sync = 1 waits and fills *info (may be NULL). */
+int hydro2d_step_f64(const double *d_rhoE, const double *d_uv, double *d_rhoE_next, double *d_uv_next,
+                     double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma, double K,
+                     size_t NB_X, size_t NB_Y, double DtDx, double DtDy, void *stream, int kernel, int sync,
+                     hydro_step_info_t *info);
+int hydro2d_step_f32(const float *d_rhoE, const float *d_uv, float *d_rhoE_next, float *d_uv_next, float *Dt_next,
+                     float C_min, float gamma, float gamma_minus_one, float divgamma, float K, size_t NB_X,
+                     size_t NB_Y, float DtDx, float DtDy, void *stream, int kernel, int sync,
+                     hydro_step_info_t *info);
+int hydro3d_step_f64(const double *d_rhoE, const double *d_uvw, double *d_rhoE_next, double *d_uvw_next,
+                     double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma, double K,
+                     size_t NB_X, size_t NB_Y, size_t NB_Z, double DtDx, double DtDy, double DtDz, void *stream,
+                     int kernel, int sync, hydro_step_info_t *info);
+int hydro3d_step_f32(const float *d_rhoE, const float *d_uvw, float *d_rhoE_next, float *d_uvw_next,
+                     float *Dt_next, float C_min, float gamma, float gamma_minus_one, float divgamma, float K,
+                     size_t NB_X, size_t NB_Y, size_t NB_Z, float DtDx, float DtDy, float DtDz, void *stream,
+                     int kernel, int sync, hydro_step_info_t *info);
+
+/* Results of the last step launched on the current device, for steps enqueued with
+ * sync = 0: valid once the caller has synchronised that step's stream. Returns
+ * HYDRO_OK, HYDRO_ERR_NONPHYSICAL or HYDRO_ERR_TIMEOUT from the step's error bits.
+ * No counterpart in the reference (its launcher is synchronous and reports nothing). */
+int hydro_last_step_info(hydro_step_info_t *info);
+
+/* ---- initial condition and mass on the device -------------------------------------- */
+/* Blast initial condition of set_init_conditions_diffusion for one subdomain covering
+ * the domain (hydro2d/main.cxx:280-338, hydro3d/main.cxx:296-363): writes the interior
+ * (ghosts untouched) and returns the first Dt = min C_min/(c_s+|u|) in *min_dt (host).
+ * Synchronous. */
+int hydro2d_init_blast_f64(double *d_rhoE, double *d_uv, size_t NB_X, size_t NB_Y, double rho_in, double rho_out,
+                           double p_in, double p_out, double C_min, double gamma, double *min_dt, void *stream);
+int hydro2d_init_blast_f32(float *d_rhoE, float *d_uv, size_t NB_X, size_t NB_Y, float rho_in, float rho_out,
+                           float p_in, float p_out, float C_min, float gamma, float *min_dt, void *stream);
+int hydro3d_init_blast_f64(double *d_rhoE, double *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, double rho_in,
+                           double rho_out, double p_in, double p_out, double C_min, double gamma, double *min_dt,
+                           void *stream);
+int hydro3d_init_blast_f32(float *d_rhoE, float *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, float rho_in,
+                           float rho_out, float p_in, float p_out, float C_min, float gamma, float *min_dt,
+                           void *stream);
+
+/* Interior density sum (the quantity of compute_total_mass, hydro2d/main.cxx:237-265,
+ * hydro3d/main.cxx:249-281) as a compensated FP64 sum on the device; NB_Z = 0 for 2D.
+ * Synchronous; *out is host memory. */
+int hydro_mass_f64(const double *d_rhoE, size_t NB_X, size_t NB_Y, size_t NB_Z, double *out, void *stream);
+int hydro_mass_f32(const float *d_rhoE, size_t NB_X, size_t NB_Y, size_t NB_Z, double *out, void *stream);
+
+/* ---- errors -------------------------------------------------------------------------- */
+/* No counterpart in the reference (it has no status return): last error code latched
+ * by any entry point (0 = none), its message, and a reset. */
+int hydro_last_error(void);
+const char *hydro_last_error_string(void);
+void hydro_clear_error(void);
+const char *hydro_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HYDRO_B200_H */

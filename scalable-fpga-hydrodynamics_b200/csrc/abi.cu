@@ -1,0 +1,246 @@
+// extern "C" entry points declared in include/hydro_b200.h.
+#include <stdio.h>
+#include <time.h>
+
+#include "../../include/hydro_b200.h"
+#include "hydro_host.h"
+
+using namespace hydro;
+
+namespace {
+
+double now_us()
+{
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec * 1e6 + ts.tv_nsec / 1e3;
+}
+
+// Select the queue's device for the duration of a call.
+struct DeviceScope {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceScope(int dev)
+    {
+        if (dev < 0) return;
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev && cudaSetDevice(dev) != cudaSuccess) {
+            set_error(kErrCuda, "cudaSetDevice(%d) failed", dev);
+            ok = false;
+        }
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// The reference never reports a status; the drop-in prints each distinct failure once
+// per call to stderr and returns a negative time for hard errors only.
+double finish_launcher(int rc, double t0, const char *what)
+{
+    const double dt = now_us() - t0;
+    if (rc == kOk) return dt;
+    fprintf(stderr, "[hydro_b200] %s: %s\n", what, last_error_string());
+    if (rc == kErrPhys) return dt; // outputs were written, as the reference would
+    return -1.0;
+}
+
+template <class T> Phys<T> phys(T C_min, T gamma, T gm1, T divgamma, T K) { return Phys<T>{C_min, gamma, gm1, divgamma, K}; }
+
+void fill(hydro_step_info_t *out, const StepInfo &in)
+{
+    if (!out) return;
+    out->mass = in.mass;
+    out->max_speed = in.max_speed;
+    out->err = in.err;
+    out->kernel = in.kernel;
+}
+
+} // namespace
+
+extern "C" {
+
+double hydro2d_launcher_f64(const double *d_rhoE, const double *d_uv, double *d_rhoE_next, double *d_uv_next,
+                            double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma,
+                            double K, size_t NB_X, size_t NB_Y, const double *DtDx, const double *DtDy,
+                            hydro_queue_t queue)
+{
+    const double t0 = now_us();
+    DeviceScope ds(queue.device);
+    if (!ds.ok) return finish_launcher(kErrCuda, t0, "launcher");
+    if (!DtDx || !DtDy) {
+        set_error(kErrArg, "launcher: DtDx/DtDy must not be null");
+        return finish_launcher(kErrArg, t0, "launcher");
+    }
+    const int rc = step2d<double>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
+                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, *DtDx, *DtDy,
+                                  (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr);
+    return finish_launcher(rc, t0, "launcher");
+}
+
+double hydro2d_launcher_f32(const float *d_rhoE, const float *d_uv, float *d_rhoE_next, float *d_uv_next,
+                            float *Dt_next, float C_min, float gamma, float gamma_minus_one, float divgamma, float K,
+                            size_t NB_X, size_t NB_Y, const float *DtDx, const float *DtDy, hydro_queue_t queue)
+{
+    const double t0 = now_us();
+    DeviceScope ds(queue.device);
+    if (!ds.ok) return finish_launcher(kErrCuda, t0, "launcher");
+    if (!DtDx || !DtDy) {
+        set_error(kErrArg, "launcher: DtDx/DtDy must not be null");
+        return finish_launcher(kErrArg, t0, "launcher");
+    }
+    const int rc = step2d<float>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
+                                 phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, *DtDx, *DtDy,
+                                 (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr);
+    return finish_launcher(rc, t0, "launcher");
+}
+
+double hydro3d_launcher_f64(const double *d_rhoE, const double *d_uvw, double *d_rhoE_next, double *d_uvw_next,
+                            double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma,
+                            double K, size_t NB_X, size_t NB_Y, size_t NB_Z, const double *DtDx, const double *DtDy,
+                            const double *DtDz, hydro_queue_t queue)
+{
+    const double t0 = now_us();
+    DeviceScope ds(queue.device);
+    if (!ds.ok) return finish_launcher(kErrCuda, t0, "launcher");
+    if (!DtDx || !DtDy || !DtDz) {
+        set_error(kErrArg, "launcher: DtDx/DtDy/DtDz must not be null");
+        return finish_launcher(kErrArg, t0, "launcher");
+    }
+    const int rc = step3d<double>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
+                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, *DtDx, *DtDy,
+                                  *DtDz, (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr);
+    return finish_launcher(rc, t0, "launcher");
+}
+
+double hydro3d_launcher_f32(const float *d_rhoE, const float *d_uvw, float *d_rhoE_next, float *d_uvw_next,
+                            float *Dt_next, float C_min, float gamma, float gamma_minus_one, float divgamma, float K,
+                            size_t NB_X, size_t NB_Y, size_t NB_Z, const float *DtDx, const float *DtDy,
+                            const float *DtDz, hydro_queue_t queue)
+{
+    const double t0 = now_us();
+    DeviceScope ds(queue.device);
+    if (!ds.ok) return finish_launcher(kErrCuda, t0, "launcher");
+    if (!DtDx || !DtDy || !DtDz) {
+        set_error(kErrArg, "launcher: DtDx/DtDy/DtDz must not be null");
+        return finish_launcher(kErrArg, t0, "launcher");
+    }
+    const int rc = step3d<float>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
+                                 phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, *DtDx, *DtDy,
+                                 *DtDz, (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr);
+    return finish_launcher(rc, t0, "launcher");
+}
+
+int hydro2d_step_f64(const double *d_rhoE, const double *d_uv, double *d_rhoE_next, double *d_uv_next,
+                     double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma, double K,
+                     size_t NB_X, size_t NB_Y, double DtDx, double DtDy, void *stream, int kernel, int sync,
+                     hydro_step_info_t *info)
+{
+    StepInfo si;
+    const int rc = step2d<double>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
+                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, DtDx, DtDy,
+                                  (cudaStream_t)stream, (Kernel)kernel, sync != 0, &si);
+    fill(info, si);
+    return rc;
+}
+
+int hydro2d_step_f32(const float *d_rhoE, const float *d_uv, float *d_rhoE_next, float *d_uv_next, float *Dt_next,
+                     float C_min, float gamma, float gamma_minus_one, float divgamma, float K, size_t NB_X,
+                     size_t NB_Y, float DtDx, float DtDy, void *stream, int kernel, int sync,
+                     hydro_step_info_t *info)
+{
+    StepInfo si;
+    const int rc = step2d<float>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
+                                 phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, DtDx, DtDy,
+                                 (cudaStream_t)stream, (Kernel)kernel, sync != 0, &si);
+    fill(info, si);
+    return rc;
+}
+
+int hydro3d_step_f64(const double *d_rhoE, const double *d_uvw, double *d_rhoE_next, double *d_uvw_next,
+                     double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma, double K,
+                     size_t NB_X, size_t NB_Y, size_t NB_Z, double DtDx, double DtDy, double DtDz, void *stream,
+                     int kernel, int sync, hydro_step_info_t *info)
+{
+    StepInfo si;
+    const int rc = step3d<double>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
+                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, DtDx, DtDy,
+                                  DtDz, (cudaStream_t)stream, (Kernel)kernel, sync != 0, &si);
+    fill(info, si);
+    return rc;
+}
+
+int hydro3d_step_f32(const float *d_rhoE, const float *d_uvw, float *d_rhoE_next, float *d_uvw_next,
+                     float *Dt_next, float C_min, float gamma, float gamma_minus_one, float divgamma, float K,
+                     size_t NB_X, size_t NB_Y, size_t NB_Z, float DtDx, float DtDy, float DtDz, void *stream,
+                     int kernel, int sync, hydro_step_info_t *info)
+{
+    StepInfo si;
+    const int rc = step3d<float>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
+                                 phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, DtDx, DtDy, DtDz,
+                                 (cudaStream_t)stream, (Kernel)kernel, sync != 0, &si);
+    fill(info, si);
+    return rc;
+}
+
+int hydro2d_init_blast_f64(double *d_rhoE, double *d_uv, size_t NB_X, size_t NB_Y, double rho_in, double rho_out,
+                           double p_in, double p_out, double C_min, double gamma, double *min_dt, void *stream)
+{
+    return init2d<double>(d_rhoE, d_uv, NB_X, NB_Y, rho_in, rho_out, p_in, p_out, C_min, gamma, min_dt,
+                          (cudaStream_t)stream);
+}
+int hydro2d_init_blast_f32(float *d_rhoE, float *d_uv, size_t NB_X, size_t NB_Y, float rho_in, float rho_out,
+                           float p_in, float p_out, float C_min, float gamma, float *min_dt, void *stream)
+{
+    return init2d<float>(d_rhoE, d_uv, NB_X, NB_Y, rho_in, rho_out, p_in, p_out, C_min, gamma, min_dt,
+                         (cudaStream_t)stream);
+}
+int hydro3d_init_blast_f64(double *d_rhoE, double *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, double rho_in,
+                           double rho_out, double p_in, double p_out, double C_min, double gamma, double *min_dt,
+                           void *stream)
+{
+    return init3d<double>(d_rhoE, d_uvw, NB_X, NB_Y, NB_Z, rho_in, rho_out, p_in, p_out, C_min, gamma, min_dt,
+                          (cudaStream_t)stream);
+}
+int hydro3d_init_blast_f32(float *d_rhoE, float *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, float rho_in,
+                           float rho_out, float p_in, float p_out, float C_min, float gamma, float *min_dt,
+                           void *stream)
+{
+    return init3d<float>(d_rhoE, d_uvw, NB_X, NB_Y, NB_Z, rho_in, rho_out, p_in, p_out, C_min, gamma, min_dt,
+                         (cudaStream_t)stream);
+}
+
+int hydro_mass_f64(const double *d_rhoE, size_t NB_X, size_t NB_Y, size_t NB_Z, double *out, void *stream)
+{
+    return mass_sum<double>(d_rhoE, NB_X, NB_Y, NB_Z, out, (cudaStream_t)stream);
+}
+int hydro_mass_f32(const float *d_rhoE, size_t NB_X, size_t NB_Y, size_t NB_Z, double *out, void *stream)
+{
+    return mass_sum<float>(d_rhoE, NB_X, NB_Y, NB_Z, out, (cudaStream_t)stream);
+}
+
+int hydro_last_step_info(hydro_step_info_t *info)
+{
+    int err;
+    DevCtx *c = ctx_current(&err);
+    if (!c) return err;
+    if (!info) return kErrArg;
+    const StepStatus st = read_status(c->status_h);
+    info->mass = st.mass + st.mass_comp;
+    info->max_speed = st.max_speed;
+    info->err = st.err;
+    info->kernel = c->last_kernel;
+    if (st.err & kErrWaitTimeout) {
+        c->dirty = true;
+        return kErrTimeout;
+    }
+    return (st.err & kErrNonPhysical) ? kErrPhys : kOk;
+}
+
+int hydro_last_error(void) { return last_error(); }
+const char *hydro_last_error_string(void) { return last_error_string(); }
+void hydro_clear_error(void) { clear_error(); }
+const char *hydro_version(void) { return "hydro_b200 0.1 (sm_100a)"; }
+
+} // extern "C"

@@ -1,0 +1,515 @@
+// 2D finite-volume step on B200: the device replacement of kernel_hydro_fvm
+// (hydro2d/kernel.cxx:132-319).
+//
+// Data layout (fixed by the reference host, hydro2d/main.cxx:80-81,120-128): the grid
+// is (NB_X+2) x (NB_Y+2) cells, row-major with Y fastest, c = i*(NB_Y+2) + j. Two
+// arrays of interleaved pairs: rhoE[c] = (rho, E), uv[c] = (rho*u, rho*v), i.e. one
+// 16-byte (FP64) or 8-byte (FP32) vector per cell per array.
+//
+// Boundaries: X is periodic by in-kernel wrap (row 0 reads row NB_X, row NB_X+1 reads
+// row 1: the single-rank ghost copy of hydro2d/main.cxx:349-378 done by addressing),
+// so the ghost rows of the input are never read. Y walls are reflective: the face
+// flux at j=1/2 and j=NB_Y+1/2 uses the mirrored state of the wall cell
+// (hydro2d/kernel.cxx:212-251).
+//
+// Kernels:
+//  strip2d   one CTA = 128 lanes over 128 consecutive columns (126 interior + one
+//            halo column each side), marching down `chunk` rows. Each row arrives in
+//            shared memory through two TMA tile loads (one per array) into a 4-deep
+//            mbarrier ring; each lane converts its cell to primitives once, computes
+//            the x face above it and the y face to its right once (neighbours via warp
+//            shuffles, warp edges via shared memory), updates the row above, stores it
+//            with 128-bit stores and folds speed and mass into the fused epilogue.
+//  direct2d  one thread per cell, scalar loads of the 5-point stencil, every face
+//            evaluated from both sides like the reference. Any alignment, any size;
+//            used when the strip kernel's TMA rules do not hold and as a cross-check.
+#include <algorithm>
+#include <stdio.h>
+
+#include "hydro_host.h"
+
+namespace hydro {
+
+template <class T> struct Args2 {
+    const T *rhoE, *uv;
+    T *rhoE_n, *uv_n;
+    T *Dt_next;
+    Phys<T> ph;
+    T DtDx, DtDy;
+    int nb_x, nb_y;
+    long long ys;
+    int chunk;
+    StepScratch *scr;
+    double2 *partials;
+    StepStatus *status;
+    unsigned seq;
+};
+
+__device__ __forceinline__ int wrap_row(int n, int nb_x) { return n == 0 ? nb_x : (n == nb_x + 1 ? 1 : n); }
+
+template <class T> __device__ __forceinline__ typename Vec2<T>::type mk2(T a, T b)
+{
+    typename Vec2<T>::type v;
+    v.x = a;
+    v.y = b;
+    return v;
+}
+
+// ------------------------------------------------------------------ direct kernel ---
+constexpr int kDirectNT = 128;
+
+template <class T> __device__ __forceinline__ Cell2<T> load_cell2(const Args2<T> &g, long long c)
+{
+    return make_cell2<T>(g.rhoE[2 * c], g.uv[2 * c], g.uv[2 * c + 1], g.rhoE[2 * c + 1], g.ph);
+}
+
+template <class T> __global__ void __launch_bounds__(kDirectNT) direct2d(Args2<T> g)
+{
+    StepAcc acc;
+    const int j = 1 + blockIdx.x * kDirectNT + threadIdx.x;
+    for (int i = 1 + blockIdx.y; i <= g.nb_x; i += gridDim.y) {
+        if (j > g.nb_y) continue;
+        const long long c = (long long)i * g.ys + j;
+        const T ur = g.rhoE[2 * c], uE = g.rhoE[2 * c + 1], uu = g.uv[2 * c], uv = g.uv[2 * c + 1];
+        const Cell2<T> P = make_cell2<T>(ur, uu, uv, uE, g.ph);
+        const Cell2<T> PL = load_cell2(g, (long long)wrap_row(i - 1, g.nb_x) * g.ys + j);
+        const Cell2<T> PR = load_cell2(g, (long long)wrap_row(i + 1, g.nb_x) * g.ys + j);
+        const Flux2<T> fx1 = face_flux(face_x(PL), face_x(P), g.ph);
+        const Flux2<T> fx2 = face_flux(face_x(P), face_x(PR), g.ph);
+        const FaceIn<T> me = face_y(P);
+        const FaceIn<T> lo = (j == 1) ? mirror(me) : face_y(load_cell2(g, c - 1));
+        const FaceIn<T> hi = (j == g.nb_y) ? mirror(me) : face_y(load_cell2(g, c + 1));
+        const Flux2<T> fy1 = face_flux(lo, me, g.ph);
+        const Flux2<T> fy2 = face_flux(me, hi, g.ph);
+        const Upd2<T> o = update2(ur, uu, uv, uE, fx1, fx2, fy1, fy2, g.DtDx, g.DtDy, g.ph);
+        g.rhoE_n[2 * c] = o.r;
+        g.rhoE_n[2 * c + 1] = o.E;
+        g.uv_n[2 * c] = o.u;
+        g.uv_n[2 * c + 1] = o.v;
+        acc.add_cell(o.r, o.speed);
+    }
+    step_epilogue<kDirectNT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y, blockIdx.x + blockIdx.y * gridDim.x,
+                                g.ph.C_min, g.Dt_next, g.status, g.seq);
+}
+
+// ------------------------------------------------------------------- strip kernel ---
+constexpr int kStripNT = 128;
+constexpr int kStripW = kStripNT - 2; // interior columns per strip
+constexpr int kStages = 4;
+
+template <class T>
+__global__ void __launch_bounds__(kStripNT, 3)
+    strip2d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args2<T> g)
+{
+    using V2 = typename Vec2<T>::type;
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr uint32_t kStageBytes = 2u * kStripNT * sizeof(V2);
+    __shared__ __align__(128) V2 sr[kStages][kStripNT];
+    __shared__ __align__(128) V2 su[kStages][kStripNT];
+    __shared__ __align__(8) uint64_t full[kStages];
+    __shared__ T xP[kStripNT / 32][7];
+    __shared__ T xF[kStripNT / 32][4];
+    __shared__ int s_abort;
+
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int jbase = kStripW * blockIdx.x; // column held by lane 0
+    const int j = jbase + t;
+    const int i0 = 1 + g.chunk * blockIdx.y;
+    const int i1 = min(i0 + g.chunk - 1, g.nb_x);
+    const int nrows = i1 - i0 + 3; // with one halo row above and below
+    const bool interior = (t >= 1) && (t <= kStripW) && (j <= g.nb_y);
+    const int xcoord = 2 * jbase;
+
+    if (t == 0) {
+        prefetch_tensormap(&tmr);
+        prefetch_tensormap(&tmu);
+        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+    auto issue = [&](int m) {
+        const int s = m % kStages;
+        const int row = wrap_row(i0 - 1 + m, g.nb_x);
+        mbar_arrive_expect_tx(&full[s], kStageBytes);
+        tma_load_2d(&sr[s][0], &tmr, xcoord, row, &full[s]);
+        tma_load_2d(&su[s][0], &tmu, xcoord, row, &full[s]);
+    };
+    if (t == 0)
+        for (int m = 0; m < kStages && m < nrows; ++m) issue(m);
+
+    StepAcc acc;
+    Cell2<T> Pm{};
+    T Ur = 0, Uu = 0, Uv = 0, UE = 0;
+    Flux2<T> fxlo{}, fyl{}, fyr{};
+    int m = 0;
+    for (; m < nrows; ++m) {
+        const int s = m % kStages;
+        if (!mbar_wait_bounded(&full[s], (m / kStages) & 1)) s_abort = 1;
+        const V2 a = sr[s][t], b = su[s][t];
+        const Cell2<T> P = make_cell2<T>(a.x, b.x, b.y, a.y, g.ph);
+        const bool yrow = (m >= 1) && (m <= nrows - 2);
+        if (yrow && lane == 0) {
+            T *x = xP[warp];
+            x[0] = P.r; x[1] = P.v; x[2] = P.p; x[3] = P.a; x[4] = P.mv; x[5] = P.mu; x[6] = P.eup;
+        }
+        __syncthreads(); // stage s consumed by every lane; warp-edge primitives published
+        if (s_abort) break;
+        if (t == 0 && m + kStages < nrows) issue(m + kStages);
+
+        if (m >= 1) {
+            const Flux2<T> fxhi = face_flux(face_x(Pm), face_x(P), g.ph);
+            if (m >= 2 && interior) {
+                const Upd2<T> o = update2(Ur, Uu, Uv, UE, fxlo, fxhi, fyl, fyr, g.DtDx, g.DtDy, g.ph);
+                const long long c = (long long)(i0 + m - 2) * g.ys + j;
+                reinterpret_cast<V2 *>(g.rhoE_n)[c] = mk2<T>(o.r, o.E);
+                reinterpret_cast<V2 *>(g.uv_n)[c] = mk2<T>(o.u, o.v);
+                acc.add_cell(o.r, o.speed);
+            }
+            fxlo = fxhi;
+        }
+        if (yrow) {
+            const FaceIn<T> me = face_y(P);
+            FaceIn<T> nb;
+            nb.r = __shfl_down_sync(FULL, me.r, 1);
+            nb.un = __shfl_down_sync(FULL, me.un, 1);
+            nb.p = __shfl_down_sync(FULL, me.p, 1);
+            nb.a = __shfl_down_sync(FULL, me.a, 1);
+            nb.mn = __shfl_down_sync(FULL, me.mn, 1);
+            nb.mt = __shfl_down_sync(FULL, me.mt, 1);
+            nb.eup = __shfl_down_sync(FULL, me.eup, 1);
+            if (lane == 31 && warp + 1 < kStripNT / 32) {
+                const T *x = xP[warp + 1];
+                nb = FaceIn<T>{x[0], x[1], x[2], x[3], x[4], x[5], x[6]};
+            }
+            FaceIn<T> L = me, R = nb;
+            if (j == 0) L = mirror(nb);        // wall at j = 1/2
+            if (j == g.nb_y) R = mirror(me);   // wall at j = NB_Y + 1/2
+            const Flux2<T> f = face_flux(L, R, g.ph);
+            if (lane == 31) {
+                T *x = xF[warp];
+                x[0] = f.r; x[1] = f.n; x[2] = f.t; x[3] = f.E;
+            }
+            __syncthreads(); // warp-edge face fluxes published
+            fyr = f;
+            fyl.r = __shfl_up_sync(FULL, f.r, 1);
+            fyl.n = __shfl_up_sync(FULL, f.n, 1);
+            fyl.t = __shfl_up_sync(FULL, f.t, 1);
+            fyl.E = __shfl_up_sync(FULL, f.E, 1);
+            if (lane == 0 && warp > 0) {
+                const T *x = xF[warp - 1];
+                fyl = Flux2<T>{x[0], x[1], x[2], x[3]};
+            }
+        }
+        Pm = P;
+        Ur = a.x; Uu = b.x; Uv = b.y; UE = a.y;
+    }
+    if (m < nrows) {
+        // gave up on a barrier: wait (bounded) for the loads still in flight before the
+        // block's shared memory is released, and report the time-out
+        acc.err |= kErrWaitTimeout;
+        if (t == 0)
+            for (int q = m; q < nrows && q < m + kStages; ++q)
+                (void)mbar_wait_bounded(&full[q % kStages], (q / kStages) & 1);
+        __syncthreads();
+    }
+    step_epilogue<kStripNT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y, blockIdx.x + blockIdx.y * gridDim.x,
+                               g.ph.C_min, g.Dt_next, g.status, g.seq);
+}
+
+// ------------------------------------------------------------- initial condition ---
+// hydro2d/main.cxx:280-338: rho = u_in inside the circle of radius min(cx,cy)/3
+// centred at ((NB_X+1)/2, (NB_Y+1)/2) in ghost-shifted indices, u_out outside;
+// E = p/(gamma-1); zero momentum. First Dt = min over cells of C_min/(c_s + |u|).
+template <class T>
+__global__ void init2d_kernel(T *rhoE, T *uv, int nb_x, int nb_y, long long ys, double cx, double cy, double radius,
+                              T u_in, T u_out, T p_in, T p_out, T C_min, T gamma, T gm1, unsigned long long *min_bits)
+{
+    using A = Ar<T>;
+    const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long best = ~0ull;
+    for (int i = 1 + blockIdx.y; i <= nb_x; i += gridDim.y) {
+        if (j > nb_y) break;
+        const double dx = __dsub_rn((double)i, cx), dy = __dsub_rn((double)j, cy);
+        const double d = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+        const bool in = d <= radius;
+        const T ur = in ? u_in : u_out;
+        const T uE = A::div(in ? p_in : p_out, gm1);
+        const long long c = (long long)i * ys + j;
+        rhoE[2 * c] = ur;
+        rhoE[2 * c + 1] = uE;
+        uv[2 * c] = T(0);
+        uv[2 * c + 1] = T(0);
+        const T inv = A::rcp(ur);
+        const T qu = A::mul(T(0), inv), qv = A::mul(T(0), inv);
+        const T temp = A::add(A::mul(qu, qu), A::mul(qv, qv));
+        const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
+        const T qp = A::mul(A::mul(gm1, ur), e_int);
+        const T cs = A::sqrt(A::mul(A::mul(gamma, qp), inv));
+        const T un = A::sqrt(temp);
+        const T local = A::div(C_min, A::add(cs, un));
+        const unsigned long long bits = (unsigned long long)__double_as_longlong((double)local);
+        best = bits < best ? bits : best;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, best, o);
+        best = ob < best ? ob : best;
+    }
+    if ((threadIdx.x & 31) == 0 && best != ~0ull) atomicMin(min_bits, best);
+}
+
+// ------------------------------------------------------------------ mass kernel ---
+template <class T>
+__global__ void mass_kernel(const T *rhoE, int nb_x, int nb_y, int nb_z, double2 *partials)
+{
+    // interior cells in row-major order; one compensated partial per block
+    const long long zs = nb_z > 0 ? nb_z + 2 : 1;
+    const long long ys = (long long)(nb_y + 2) * zs;
+    const long long ncol = (long long)nb_y * (nb_z > 0 ? nb_z : 1);
+    const long long n = (long long)nb_x * ncol;
+    double s = 0.0, c = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long i = 1 + q / ncol, r = q % ncol;
+        long long cell;
+        if (nb_z > 0) cell = i * ys + (1 + r / nb_z) * zs + (1 + r % nb_z);
+        else cell = i * ys + 1 + r;
+        neumaier_add(s, c, (double)rhoE[2 * cell]);
+    }
+    StepAcc acc;
+    acc.ms = s;
+    acc.mc = c;
+    // reuse the epilogue's deterministic block combine through a private path
+    __shared__ double ss[32], sc[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double s2 = __shfl_xor_sync(0xffffffffu, s, o);
+        const double c2 = __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane & o) {
+            double a = s2, b = c2;
+            neumaier_merge(a, b, s, c);
+            s = a; c = b;
+        } else {
+            neumaier_merge(s, c, s2, c2);
+        }
+    }
+    if (lane == 0) { ss[warp] = s; sc[warp] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) neumaier_merge(s, c, ss[w], sc[w]);
+        partials[blockIdx.x] = make_double2(s, c);
+    }
+}
+
+__global__ void sum_partials_kernel(const double2 *partials, int n, double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0.0, c = 0.0;
+    for (int b = 0; b < n; ++b) neumaier_merge(s, c, partials[b].x, partials[b].y);
+    *out = __dadd_rn(s, c);
+}
+
+// ----------------------------------------------------------------- host drivers ---
+namespace {
+template <class T> CUtensorMapDataType tmap_type();
+template <> CUtensorMapDataType tmap_type<double>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT64; }
+template <> CUtensorMapDataType tmap_type<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
+
+bool aligned(const void *p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+} // namespace
+
+template <class T>
+int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
+           size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info)
+{
+    if (!rhoE || !uv || !rhoE_next || !uv_next || !Dt_next) {
+        set_error(kErrArg, "step2d: null pointer argument");
+        return kErrArg;
+    }
+    if (nb_x > (1u << 30) || nb_y > (1u << 30) || (nb_x + 2) * (nb_y + 2) > (size_t(1) << 40)) {
+        set_error(kErrArg, "step2d: grid %zu x %zu too large", nb_x, nb_y);
+        return kErrArg;
+    }
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    if (nb_x == 0 || nb_y == 0) {
+        // no interior cell: the reference leaves max_speed at 0 and writes C_min / 0
+        const T dt = div_zero(ph.C_min);
+        cudaError_t e = cudaMemcpyAsync(Dt_next, &dt, sizeof(T), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "step2d: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        if (info) *info = StepInfo{};
+        return kOk;
+    }
+    if (ctx->dirty) {
+        cudaMemsetAsync(ctx->scr, 0, sizeof(StepScratch), stream);
+        ctx->dirty = false;
+    }
+
+    Args2<T> g;
+    g.rhoE = rhoE; g.uv = uv; g.rhoE_n = rhoE_next; g.uv_n = uv_next; g.Dt_next = Dt_next;
+    g.ph = ph; g.DtDx = DtDx; g.DtDy = DtDy;
+    g.nb_x = (int)nb_x; g.nb_y = (int)nb_y; g.ys = (long long)nb_y + 2;
+    g.scr = ctx->scr; g.status = ctx->status_d; g.seq = ++ctx->seq;
+
+    using V2 = typename Vec2<T>::type;
+    const size_t rowbytes = 2 * sizeof(T) * (nb_y + 2);
+    bool strip_ok = aligned(rhoE, 16) && aligned(uv, 16) && aligned(rhoE_next, sizeof(V2)) &&
+                    aligned(uv_next, sizeof(V2)) && rowbytes % 16 == 0;
+    CUtensorMap tmr, tmu;
+    if (strip_ok && which != Kernel::Direct) {
+        strip_ok = encode_tmap_2d(&tmr, tmap_type<T>(), rhoE, 2 * (nb_y + 2), nb_x + 2, rowbytes, 2 * kStripNT, 1) &&
+                   encode_tmap_2d(&tmu, tmap_type<T>(), uv, 2 * (nb_y + 2), nb_x + 2, rowbytes, 2 * kStripNT, 1);
+    }
+    if (which == Kernel::Strip && !strip_ok) {
+        set_error(kErrArg, "step2d: strip kernel needs 16-byte aligned arrays and rows");
+        return kErrArg;
+    }
+    const bool use_strip = strip_ok && which != Kernel::Direct;
+
+    cudaError_t e;
+    unsigned nblocks;
+    if (use_strip) {
+        const int nstrips = (int)((nb_y + kStripW - 1) / kStripW);
+        const int target = 148 * 3 * 8;
+        int nchunks = (target + nstrips - 1) / nstrips;
+        int chunk = (int)((nb_x + nchunks - 1) / nchunks);
+        chunk = std::min(256, std::max(16, chunk));
+        nchunks = (int)((nb_x + chunk - 1) / chunk);
+        if (nchunks > 65535) {
+            chunk = (int)((nb_x + 65534) / 65535);
+            nchunks = (int)((nb_x + chunk - 1) / chunk);
+        }
+        g.chunk = chunk;
+        nblocks = (unsigned)nstrips * (unsigned)nchunks;
+        if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
+        g.partials = ctx->partials;
+        strip2d<T><<<dim3(nstrips, nchunks), kStripNT, 0, stream>>>(tmr, tmu, g);
+    } else {
+        const int gx = (int)((nb_y + kDirectNT - 1) / kDirectNT);
+        const int gy = (int)std::min<size_t>(nb_x, 65535);
+        nblocks = (unsigned)gx * (unsigned)gy;
+        if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
+        g.partials = ctx->partials;
+        g.chunk = 0;
+        direct2d<T><<<dim3(gx, gy), kDirectNT, 0, stream>>>(g);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        ctx->dirty = true;
+        set_error(kErrCuda, "step2d launch: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    ctx->last_kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
+    if (!sync) {
+        if (info) info->kernel = ctx->last_kernel;
+        return kOk;
+    }
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        ctx->dirty = true;
+        set_error(kErrCuda, "step2d: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    const StepStatus st = read_status(ctx->status_h);
+    if (info) {
+        info->mass = st.mass + st.mass_comp;
+        info->max_speed = st.max_speed;
+        info->err = st.err;
+        info->kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
+    }
+    if (st.err & kErrWaitTimeout) {
+        ctx->dirty = true;
+        set_error(kErrTimeout, "step2d: a TMA barrier wait timed out");
+        return kErrTimeout;
+    }
+    if (st.err & kErrNonPhysical) {
+        set_error(kErrPhys, "step2d: non-physical state (rho <= 0 or non-finite signal speed)");
+        return kErrPhys;
+    }
+    return kOk;
+}
+
+template <class T>
+int init2d(T *rhoE, T *uv, size_t nb_x, size_t nb_y, T u_in, T u_out, T p_in, T p_out, T C_min, T gamma,
+           T *min_dt, cudaStream_t stream)
+{
+    if (!rhoE || !uv || !min_dt || nb_x == 0 || nb_y == 0 || nb_x > (1u << 30) || nb_y > (1u << 30)) {
+        set_error(kErrArg, "init2d: invalid argument");
+        return kErrArg;
+    }
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    unsigned long long *bits = &ctx->scr->max_bits; // borrowed while no step is in flight
+    const T big = T(1e20);
+    const unsigned long long init = (unsigned long long)__builtin_bit_cast(long long, (double)big);
+    const double cx = double(nb_x + 1) / 2.0, cy = double(nb_y + 1) / 2.0;
+    const double radius = std::min(cx, cy) / 3;
+    const T gm1 = gamma - T(1);
+    cudaError_t e = cudaMemcpyAsync(bits, &init, sizeof init, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+        const int gx = (int)((nb_y + 127) / 128), gy = (int)std::min<size_t>(nb_x, 65535);
+        init2d_kernel<T><<<dim3(gx, gy), 128, 0, stream>>>(rhoE, uv, (int)nb_x, (int)nb_y, (long long)nb_y + 2, cx, cy,
+                                                           radius, u_in, u_out, p_in, p_out, C_min, gamma, gm1, bits);
+        e = cudaGetLastError();
+    }
+    unsigned long long res = 0;
+    const unsigned long long zero = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&res, bits, sizeof res, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(bits, &zero, sizeof zero, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "init2d: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    *min_dt = (T)__builtin_bit_cast(double, (long long)res);
+    return kOk;
+}
+
+template <class T> int mass_sum(const T *rhoE, size_t nb_x, size_t nb_y, size_t nb_z, double *out, cudaStream_t s)
+{
+    if (!rhoE || !out) {
+        set_error(kErrArg, "mass_sum: null pointer");
+        return kErrArg;
+    }
+    if (nb_x == 0 || nb_y == 0) {
+        *out = 0.0;
+        return kOk;
+    }
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    const int nb = 148 * 8;
+    if ((err = ctx_reserve(ctx, nb + 1)) != kOk) return err;
+    double *dres = reinterpret_cast<double *>(ctx->partials + nb);
+    mass_kernel<T><<<nb, 256, 0, s>>>(rhoE, (int)nb_x, (int)nb_y, (int)nb_z, ctx->partials);
+    sum_partials_kernel<<<1, 32, 0, s>>>(ctx->partials, nb, dres);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dres, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "mass_sum: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    return kOk;
+}
+
+template int step2d<double>(const double *, const double *, double *, double *, double *, const Phys<double> &,
+                            size_t, size_t, double, double, cudaStream_t, Kernel, bool, StepInfo *);
+template int step2d<float>(const float *, const float *, float *, float *, float *, const Phys<float> &, size_t,
+                           size_t, float, float, cudaStream_t, Kernel, bool, StepInfo *);
+template int init2d<double>(double *, double *, size_t, size_t, double, double, double, double, double, double,
+                            double *, cudaStream_t);
+template int init2d<float>(float *, float *, size_t, size_t, float, float, float, float, float, float, float *,
+                           cudaStream_t);
+template int mass_sum<double>(const double *, size_t, size_t, size_t, double *, cudaStream_t);
+template int mass_sum<float>(const float *, size_t, size_t, size_t, double *, cudaStream_t);
+
+} // namespace hydro

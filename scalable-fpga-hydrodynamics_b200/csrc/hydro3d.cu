@@ -1,0 +1,446 @@
+// 3D finite-volume step on B200: the device replacement of kernel_hydro3d_fvm
+// (hydro3d/kernel.cxx:145-407).
+//
+// Layout (hydro3d/main.cxx:80-87,120-130): (NB_X+2)(NB_Y+2)(NB_Z+2) cells, Z fastest,
+// c = i*(NB_Y+2)(NB_Z+2) + j*(NB_Z+2) + k; rhoE[c] = (rho, E) pairs and
+// uvw[c] = (rho*u, rho*v, rho*w) triples.
+// Boundaries: periodic X by in-kernel wrap; reflective Y and Z walls from the mirrored
+// wall cell (hydro3d/kernel.cxx:238-320).
+//
+// Kernels:
+//  strip3d   one CTA = 8 warps over an 8 (y) x 32 (z) tile of columns (6 x 30 interior
+//            plus a one-cell halo ring), marching down `chunk` X planes. Each lane copies
+//            its own cell of each plane into a 4-deep shared-memory ring with cp.async
+//            (any alignment of the interleaved pairs/triples), converts it to primitives
+//            once, and per plane computes one x face (registers), one z face (warp
+//            shuffles) and one y face (shared memory, double-buffered by plane parity,
+//            one barrier per plane), then updates the plane behind it.
+//  direct3d  one thread per cell, the 7-point stencil loaded directly, every face
+//            evaluated from both sides like the reference.
+#include <algorithm>
+#include <stdio.h>
+
+#include "hydro_host.h"
+
+namespace hydro {
+
+template <class T> struct Args3 {
+    const T *rhoE, *uvw;
+    T *rhoE_n, *uvw_n;
+    T *Dt_next;
+    Phys<T> ph;
+    T DtDx, DtDy, DtDz;
+    int nb_x, nb_y, nb_z;
+    long long zs, zy;
+    int chunk;
+    StepScratch *scr;
+    double2 *partials;
+    StepStatus *status;
+    unsigned seq;
+};
+
+__device__ __forceinline__ int wrap_plane(int n, int nb_x) { return n == 0 ? nb_x : (n == nb_x + 1 ? 1 : n); }
+
+template <class T> __device__ __forceinline__ Cell3<T> load_cell3(const Args3<T> &g, long long c)
+{
+    return make_cell3<T>(g.rhoE[2 * c], g.uvw[3 * c], g.uvw[3 * c + 1], g.uvw[3 * c + 2], g.rhoE[2 * c + 1], g.ph);
+}
+
+// ------------------------------------------------------------------ direct kernel ---
+template <class T> __global__ void __launch_bounds__(128) direct3d(Args3<T> g)
+{
+    StepAcc acc;
+    const int k = 1 + blockIdx.x * 32 + threadIdx.x;
+    const int j = 1 + blockIdx.y * 4 + threadIdx.y;
+    for (int i = 1 + blockIdx.z; i <= g.nb_x; i += gridDim.z) {
+        if (k > g.nb_z || j > g.nb_y) continue;
+        const long long c = (long long)i * g.zy + (long long)j * g.zs + k;
+        const T ur = g.rhoE[2 * c], uE = g.rhoE[2 * c + 1];
+        const T uu = g.uvw[3 * c], uv = g.uvw[3 * c + 1], uw = g.uvw[3 * c + 2];
+        const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, g.ph);
+        const long long cxm = (long long)wrap_plane(i - 1, g.nb_x) * g.zy + (long long)j * g.zs + k;
+        const long long cxp = (long long)wrap_plane(i + 1, g.nb_x) * g.zy + (long long)j * g.zs + k;
+        const Flux3<T> fx1 = face_flux3(face3_x(load_cell3(g, cxm)), face3_x(P), g.ph);
+        const Flux3<T> fx2 = face_flux3(face3_x(P), face3_x(load_cell3(g, cxp)), g.ph);
+        const FaceIn3<T> my = face3_y(P);
+        const FaceIn3<T> ylo = (j == 1) ? mirror3(my) : face3_y(load_cell3(g, c - g.zs));
+        const FaceIn3<T> yhi = (j == g.nb_y) ? mirror3(my) : face3_y(load_cell3(g, c + g.zs));
+        const Flux3<T> fy1 = face_flux3(ylo, my, g.ph);
+        const Flux3<T> fy2 = face_flux3(my, yhi, g.ph);
+        const FaceIn3<T> mz = face3_z(P);
+        const FaceIn3<T> zlo = (k == 1) ? mirror3(mz) : face3_z(load_cell3(g, c - 1));
+        const FaceIn3<T> zhi = (k == g.nb_z) ? mirror3(mz) : face3_z(load_cell3(g, c + 1));
+        const Flux3<T> fz1 = face_flux3(zlo, mz, g.ph);
+        const Flux3<T> fz2 = face_flux3(mz, zhi, g.ph);
+        const Upd3<T> o = update3(ur, uu, uv, uw, uE, fx1, fx2, fy1, fy2, fz1, fz2, g.DtDx, g.DtDy, g.DtDz, g.ph);
+        g.rhoE_n[2 * c] = o.r;
+        g.rhoE_n[2 * c + 1] = o.E;
+        g.uvw_n[3 * c] = o.u;
+        g.uvw_n[3 * c + 1] = o.v;
+        g.uvw_n[3 * c + 2] = o.w;
+        acc.add_cell(o.r, o.speed);
+    }
+    step_epilogue<128, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
+                          blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
+                          g.status, g.seq);
+}
+
+// ------------------------------------------------------------------- strip kernel ---
+constexpr int k3Warps = 8;                 // y extent of the tile (with halo)
+constexpr int k3NT = 32 * k3Warps;         // threads
+constexpr int k3TY = k3Warps - 2;          // interior rows per tile
+constexpr int k3TZ = 30;                   // interior columns per tile
+constexpr int k3Stages = 4;
+
+__device__ __forceinline__ void cp_async(void *dst, const void *src, int bytes, bool valid)
+{
+    const uint32_t d = smem_u32(dst);
+    const int n = valid ? bytes : 0;
+    if (bytes == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <class T> struct Smem3 {
+    T st[k3Stages][5][k3NT];      // per plane: rho, E, rho_u, rho_v, rho_w
+    T xP[2][8][k3NT];             // y-face inputs of each lane's cell, by plane parity
+    T xF[2][5][k3NT];             // each lane's +y face flux, by plane parity
+};
+
+template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem3<T> &S = *reinterpret_cast<Smem3<T> *>(smem_raw);
+    constexpr unsigned FULL = 0xffffffffu;
+
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int kbase = k3TZ * blockIdx.x, jbase = k3TY * blockIdx.y;
+    const int k = kbase + lane, j = jbase + w;
+    const int i0 = 1 + g.chunk * blockIdx.z;
+    const int i1 = min(i0 + g.chunk - 1, g.nb_x);
+    const int nplanes = i1 - i0 + 3;
+    const bool in_array = (j <= g.nb_y + 1) && (k <= g.nb_z + 1);
+    const bool interior = (w >= 1) && (w <= k3TY) && (lane >= 1) && (lane <= k3TZ) && (j <= g.nb_y) && (k <= g.nb_z);
+    const bool iwarp = (w >= 1) && (w <= k3TY) && (jbase + 1 <= g.nb_y); // warp holds interior rows
+    const long long colofs = (long long)j * g.zs + k;
+
+    auto issue = [&](int m) {
+        const int s = m % k3Stages;
+        if (m < nplanes) {
+            const long long c = (long long)wrap_plane(i0 - 1 + m, g.nb_x) * g.zy + colofs;
+            const T *pr = in_array ? g.rhoE + 2 * c : g.rhoE;
+            const T *pu = in_array ? g.uvw + 3 * c : g.uvw;
+            cp_async(&S.st[s][0][t], pr, sizeof(T), in_array);
+            cp_async(&S.st[s][1][t], pr + 1, sizeof(T), in_array);
+            cp_async(&S.st[s][2][t], pu, sizeof(T), in_array);
+            cp_async(&S.st[s][3][t], pu + 1, sizeof(T), in_array);
+            cp_async(&S.st[s][4][t], pu + 2, sizeof(T), in_array);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int m = 0; m < k3Stages - 1; ++m) issue(m);
+
+    StepAcc acc;
+    Cell3<T> Pm{};
+    T Ur = 0, Uu = 0, Uv = 0, Uw = 0, UE = 0;
+    Flux3<T> fxlo{};
+    for (int m = 0; m < nplanes; ++m) {
+        issue(m + k3Stages - 1);
+        cp_async_wait<k3Stages - 1>();
+        const int s = m % k3Stages;
+        const T ur = S.st[s][0][t], uE = S.st[s][1][t], uu = S.st[s][2][t], uv = S.st[s][3][t],
+                uw = S.st[s][4][t];
+        const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, g.ph);
+        {
+            const FaceIn3<T> fy = face3_y(P);
+            T *x = &S.xP[m & 1][0][t];
+            x[0 * k3NT] = fy.r; x[1 * k3NT] = fy.un; x[2 * k3NT] = fy.p; x[3 * k3NT] = fy.a;
+            x[4 * k3NT] = fy.mn; x[5 * k3NT] = fy.mt1; x[6 * k3NT] = fy.mt2; x[7 * k3NT] = fy.eup;
+        }
+        Flux3<T> fxhi{};
+        if (m >= 1 && iwarp) fxhi = face_flux3(face3_x(Pm), face3_x(P), g.ph);
+
+        // faces of plane m-1 (an interior plane when 2 <= m)
+        if (m >= 2) {
+            // +y face of (j | j+1), from this lane's previous-plane cell and the warp above's
+            const FaceIn3<T> me = face3_y(Pm);
+            Flux3<T> fy{};
+            if (w < k3Warps - 1) {
+                const T *x = &S.xP[(m - 1) & 1][0][t + 32];
+                FaceIn3<T> nb{x[0 * k3NT], x[1 * k3NT], x[2 * k3NT], x[3 * k3NT],
+                              x[4 * k3NT], x[5 * k3NT], x[6 * k3NT], x[7 * k3NT]};
+                FaceIn3<T> L = me, R = nb;
+                if (j == 0) L = mirror3(nb);
+                if (j == g.nb_y) R = mirror3(me);
+                fy = face_flux3(L, R, g.ph);
+                T *xf = &S.xF[m & 1][0][t];
+                xf[0 * k3NT] = fy.r; xf[1 * k3NT] = fy.n; xf[2 * k3NT] = fy.t1; xf[3 * k3NT] = fy.t2;
+                xf[4 * k3NT] = fy.E;
+            }
+            // +z face of (k | k+1) via shuffles within the warp
+            Flux3<T> fz{};
+            if (iwarp) {
+                const FaceIn3<T> mz = face3_z(Pm);
+                FaceIn3<T> nz;
+                nz.r = __shfl_down_sync(FULL, mz.r, 1);
+                nz.un = __shfl_down_sync(FULL, mz.un, 1);
+                nz.p = __shfl_down_sync(FULL, mz.p, 1);
+                nz.a = __shfl_down_sync(FULL, mz.a, 1);
+                nz.mn = __shfl_down_sync(FULL, mz.mn, 1);
+                nz.mt1 = __shfl_down_sync(FULL, mz.mt1, 1);
+                nz.mt2 = __shfl_down_sync(FULL, mz.mt2, 1);
+                nz.eup = __shfl_down_sync(FULL, mz.eup, 1);
+                FaceIn3<T> L = mz, R = nz;
+                if (k == 0) L = mirror3(nz);
+                if (k == g.nb_z) R = mirror3(mz);
+                fz = face_flux3(L, R, g.ph);
+            }
+            __syncthreads(); // +y faces of this plane published
+            if (iwarp) {
+                Flux3<T> fzl;
+                fzl.r = __shfl_up_sync(FULL, fz.r, 1);
+                fzl.n = __shfl_up_sync(FULL, fz.n, 1);
+                fzl.t1 = __shfl_up_sync(FULL, fz.t1, 1);
+                fzl.t2 = __shfl_up_sync(FULL, fz.t2, 1);
+                fzl.E = __shfl_up_sync(FULL, fz.E, 1);
+                if (interior) {
+                    const T *xf = &S.xF[m & 1][0][t - 32];
+                    const Flux3<T> fyl{xf[0 * k3NT], xf[1 * k3NT], xf[2 * k3NT], xf[3 * k3NT], xf[4 * k3NT]};
+                    const Upd3<T> o = update3(Ur, Uu, Uv, Uw, UE, fxlo, fxhi, fyl, fy, fzl, fz, g.DtDx, g.DtDy,
+                                              g.DtDz, g.ph);
+                    const long long c = (long long)(i0 + m - 2) * g.zy + colofs;
+                    g.rhoE_n[2 * c] = o.r;
+                    g.rhoE_n[2 * c + 1] = o.E;
+                    g.uvw_n[3 * c] = o.u;
+                    g.uvw_n[3 * c + 1] = o.v;
+                    g.uvw_n[3 * c + 2] = o.w;
+                    acc.add_cell(o.r, o.speed);
+                }
+            }
+        } else {
+            __syncthreads(); // keep one barrier per plane: publishes this plane's xP
+        }
+        fxlo = fxhi;
+        Pm = P;
+        Ur = ur; Uu = uu; Uv = uv; Uw = uw; UE = uE;
+    }
+    cp_async_wait<0>();
+    step_epilogue<k3NT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
+                           blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
+                           g.status, g.seq);
+}
+
+// ------------------------------------------------------------- initial condition ---
+// hydro3d/main.cxx:296-363
+template <class T>
+__global__ void init3d_kernel(T *rhoE, T *uvw, int nb_x, int nb_y, int nb_z, long long zs, long long zy, double cx,
+                              double cy, double cz, double radius, T u_in, T u_out, T p_in, T p_out, T C_min,
+                              T gamma, T gm1, unsigned long long *min_bits)
+{
+    using A = Ar<T>;
+    const int k = 1 + blockIdx.x * 32 + threadIdx.x;
+    const int j = 1 + blockIdx.y * 4 + threadIdx.y;
+    unsigned long long best = ~0ull;
+    if (k <= nb_z && j <= nb_y) {
+        for (int i = 1 + blockIdx.z; i <= nb_x; i += gridDim.z) {
+            const double dx = __dsub_rn((double)i, cx), dy = __dsub_rn((double)j, cy), dz = __dsub_rn((double)k, cz);
+            const double d =
+                __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+            const bool in = d <= radius;
+            const T ur = in ? u_in : u_out;
+            const T uE = A::div(in ? p_in : p_out, gm1);
+            const long long c = (long long)i * zy + (long long)j * zs + k;
+            rhoE[2 * c] = ur;
+            rhoE[2 * c + 1] = uE;
+            uvw[3 * c] = T(0);
+            uvw[3 * c + 1] = T(0);
+            uvw[3 * c + 2] = T(0);
+            const T inv = A::rcp(ur);
+            const T q = A::mul(T(0), inv);
+            const T temp = A::add(A::add(A::mul(q, q), A::mul(q, q)), A::mul(q, q));
+            const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
+            const T qp = A::mul(A::mul(gm1, ur), e_int);
+            const T cs = A::sqrt(A::mul(A::mul(gamma, qp), inv));
+            const T un = A::sqrt(temp);
+            const T local = A::div(C_min, A::add(cs, un));
+            const unsigned long long bits = (unsigned long long)__double_as_longlong((double)local);
+            best = bits < best ? bits : best;
+        }
+    }
+    const int tl = threadIdx.x + 32 * threadIdx.y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, best, o);
+        best = ob < best ? ob : best;
+    }
+    if ((tl & 31) == 0 && best != ~0ull) atomicMin(min_bits, best);
+}
+
+// ----------------------------------------------------------------- host drivers ---
+template <class T>
+int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
+           size_t nb_y, size_t nb_z, T DtDx, T DtDy, T DtDz, cudaStream_t stream, Kernel which, bool sync,
+           StepInfo *info)
+{
+    if (!rhoE || !uvw || !rhoE_next || !uvw_next || !Dt_next) {
+        set_error(kErrArg, "step3d: null pointer argument");
+        return kErrArg;
+    }
+    if (nb_x > (1u << 30) || nb_y > (1u << 30) || nb_z > (1u << 30) ||
+        (double)(nb_x + 2) * (nb_y + 2) * (nb_z + 2) > 1.0e12) {
+        set_error(kErrArg, "step3d: grid %zu x %zu x %zu too large", nb_x, nb_y, nb_z);
+        return kErrArg;
+    }
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    if (nb_x == 0 || nb_y == 0 || nb_z == 0) {
+        const T dt = div_zero(ph.C_min);
+        cudaError_t e = cudaMemcpyAsync(Dt_next, &dt, sizeof(T), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "step3d: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        if (info) *info = StepInfo{};
+        return kOk;
+    }
+    if (ctx->dirty) {
+        cudaMemsetAsync(ctx->scr, 0, sizeof(StepScratch), stream);
+        ctx->dirty = false;
+    }
+    Args3<T> g;
+    g.rhoE = rhoE; g.uvw = uvw; g.rhoE_n = rhoE_next; g.uvw_n = uvw_next; g.Dt_next = Dt_next;
+    g.ph = ph; g.DtDx = DtDx; g.DtDy = DtDy; g.DtDz = DtDz;
+    g.nb_x = (int)nb_x; g.nb_y = (int)nb_y; g.nb_z = (int)nb_z;
+    g.zs = (long long)nb_z + 2; g.zy = (long long)(nb_y + 2) * g.zs;
+    g.scr = ctx->scr; g.status = ctx->status_d; g.seq = ++ctx->seq;
+
+    const bool use_strip = which != Kernel::Direct;
+    unsigned nblocks;
+    if (use_strip) {
+        const int nz = (int)((nb_z + k3TZ - 1) / k3TZ), ny = (int)((nb_y + k3TY - 1) / k3TY);
+        if (ny > 65535) {
+            set_error(kErrArg, "step3d: NB_Y %zu too large for the strip kernel", nb_y);
+            return kErrArg;
+        }
+        const int target = 148 * 2 * 8;
+        int nchunks = std::max(1, (target + nz * ny - 1) / (nz * ny));
+        int chunk = (int)((nb_x + nchunks - 1) / nchunks);
+        chunk = std::min(256, std::max(8, chunk));
+        nchunks = (int)((nb_x + chunk - 1) / chunk);
+        if (nchunks > 65535) {
+            chunk = (int)((nb_x + 65534) / 65535);
+            nchunks = (int)((nb_x + chunk - 1) / chunk);
+        }
+        g.chunk = chunk;
+        nblocks = (unsigned)nz * ny * nchunks;
+        if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
+        g.partials = ctx->partials;
+        const int smem = (int)sizeof(Smem3<T>);
+        static bool attr_set[2] = {false, false};
+        bool &done = attr_set[sizeof(T) == 8];
+        if (!done) {
+            cudaFuncSetAttribute(strip3d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            done = true;
+        }
+        strip3d<T><<<dim3(nz, ny, nchunks), k3NT, smem, stream>>>(g);
+    } else {
+        const int gx = (int)((nb_z + 31) / 32), gy = (int)((nb_y + 3) / 4), gz = (int)std::min<size_t>(nb_x, 65535);
+        if (gy > 65535) {
+            set_error(kErrArg, "step3d: NB_Y %zu too large", nb_y);
+            return kErrArg;
+        }
+        nblocks = (unsigned)gx * gy * gz;
+        if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
+        g.partials = ctx->partials;
+        g.chunk = 0;
+        direct3d<T><<<dim3(gx, gy, gz), dim3(32, 4), 0, stream>>>(g);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        ctx->dirty = true;
+        set_error(kErrCuda, "step3d launch: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    ctx->last_kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
+    if (!sync) {
+        if (info) info->kernel = ctx->last_kernel;
+        return kOk;
+    }
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        ctx->dirty = true;
+        set_error(kErrCuda, "step3d: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    const StepStatus st = read_status(ctx->status_h);
+    if (info) {
+        info->mass = st.mass + st.mass_comp;
+        info->max_speed = st.max_speed;
+        info->err = st.err;
+        info->kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
+    }
+    if (st.err & kErrNonPhysical) {
+        set_error(kErrPhys, "step3d: non-physical state (rho <= 0 or non-finite signal speed)");
+        return kErrPhys;
+    }
+    return kOk;
+}
+
+template <class T>
+int init3d(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, T u_in, T u_out, T p_in, T p_out, T C_min,
+           T gamma, T *min_dt, cudaStream_t stream)
+{
+    if (!rhoE || !uvw || !min_dt || nb_x == 0 || nb_y == 0 || nb_z == 0 || nb_x > (1u << 30) ||
+        (nb_y + 3) / 4 > 65535) {
+        set_error(kErrArg, "init3d: invalid argument");
+        return kErrArg;
+    }
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    unsigned long long *bits = &ctx->scr->max_bits;
+    const T big = T(1e20);
+    const unsigned long long init = (unsigned long long)__builtin_bit_cast(long long, (double)big);
+    const double cx = double(nb_x + 1) / 2.0, cy = double(nb_y + 1) / 2.0, cz = double(nb_z + 1) / 2.0;
+    const double radius = std::min({cx, cy, cz}) / 3;
+    const T gm1 = gamma - T(1);
+    cudaError_t e = cudaMemcpyAsync(bits, &init, sizeof init, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+        const long long zs = (long long)nb_z + 2, zy = (long long)(nb_y + 2) * zs;
+        dim3 grid((unsigned)((nb_z + 31) / 32), (unsigned)((nb_y + 3) / 4), (unsigned)std::min<size_t>(nb_x, 65535));
+        init3d_kernel<T><<<grid, dim3(32, 4), 0, stream>>>(rhoE, uvw, (int)nb_x, (int)nb_y, (int)nb_z, zs, zy, cx, cy,
+                                                           cz, radius, u_in, u_out, p_in, p_out, C_min, gamma, gm1,
+                                                           bits);
+        e = cudaGetLastError();
+    }
+    unsigned long long res = 0;
+    const unsigned long long zero = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&res, bits, sizeof res, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(bits, &zero, sizeof zero, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "init3d: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    *min_dt = (T)__builtin_bit_cast(double, (long long)res);
+    return kOk;
+}
+
+template int step3d<double>(const double *, const double *, double *, double *, double *, const Phys<double> &,
+                            size_t, size_t, size_t, double, double, double, cudaStream_t, Kernel, bool, StepInfo *);
+template int step3d<float>(const float *, const float *, float *, float *, float *, const Phys<float> &, size_t,
+                           size_t, size_t, float, float, float, cudaStream_t, Kernel, bool, StepInfo *);
+template int init3d<double>(double *, double *, size_t, size_t, size_t, double, double, double, double, double,
+                            double, double *, cudaStream_t);
+template int init3d<float>(float *, float *, size_t, size_t, size_t, float, float, float, float, float, float,
+                           float *, cudaStream_t);
+
+} // namespace hydro

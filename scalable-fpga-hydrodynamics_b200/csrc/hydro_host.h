@@ -1,0 +1,112 @@
+// Host-side runtime of the CUDA library: per-device contexts (scratch words, the
+// host-mapped status record), the error latch behind hydro_last_error(), TMA
+// descriptor encoding, and the typed step entry points the C ABI forwards to.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "hydro_rt.cuh"
+
+namespace hydro {
+
+// Which kernel a step runs.
+enum class Kernel : int {
+    Auto = 0,   // strip kernel when its alignment rules hold, else the direct kernel
+    Strip = 1,  // TMA-fed strip march (faces computed once)
+    Direct = 2, // one thread per cell, neighbours loaded directly (faces computed twice)
+};
+
+struct DevCtx {
+    int device = -1;
+    StepScratch *scr = nullptr;   // device
+    double2 *partials = nullptr;  // device, one per block
+    size_t partial_cap = 0;
+    StepStatus *status_h = nullptr; // host-mapped
+    StepStatus *status_d = nullptr; // device alias of status_h
+    unsigned seq = 0;
+    int last_kernel = 0; // Kernel run by the last step launch
+    bool dirty = false; // a launch failed: scratch words must be re-zeroed
+};
+
+// Copy of the host-mapped status record, read field by field through volatile loads.
+inline StepStatus read_status(const StepStatus *p)
+{
+    const volatile StepStatus *v = p;
+    StepStatus s;
+    s.mass = v->mass;
+    s.mass_comp = v->mass_comp;
+    s.max_speed = v->max_speed;
+    s.err = v->err;
+    s.seq = v->seq;
+    return s;
+}
+
+// a / 0 evaluated at run time (the reference's Dt_next when no cell exists)
+template <class T> inline T div_zero(T a)
+{
+    volatile T z = T(0);
+    return a / z;
+}
+
+// Context of the current device (created on first use; never freed before exit).
+DevCtx *ctx_current(int *err);
+// Grow the partials array to at least n entries (synchronises the device on growth).
+int ctx_reserve(DevCtx *c, size_t n);
+
+// error latch (process-wide, last error wins)
+void set_error(int code, const char *fmt, ...);
+int last_error();
+const char *last_error_string();
+void clear_error();
+
+// return codes of the typed entry points
+enum : int {
+    kOk = 0,
+    kErrArg = -1,   // invalid argument (sizes, null pointers)
+    kErrCuda = -2,  // a CUDA runtime call failed
+    kErrPhys = -3,  // the step produced a non-physical state (flag only; outputs written)
+    kErrTimeout = -4,
+};
+
+// Encode a 2D tiled tensor map (no swizzle, zero OOB fill). Returns false when the
+// driver entry point is missing or encoding fails.
+bool encode_tmap_2d(CUtensorMap *tm, CUtensorMapDataType dt, const void *base, uint64_t dim0, uint64_t dim1,
+                    uint64_t stride1_bytes, uint32_t box0, uint32_t box1);
+bool encode_tmap_3d(CUtensorMap *tm, CUtensorMapDataType dt, const void *base, uint64_t dim0, uint64_t dim1,
+                    uint64_t dim2, uint64_t stride1_bytes, uint64_t stride2_bytes, uint32_t box0, uint32_t box1,
+                    uint32_t box2);
+
+// Result of one step beyond the outputs the reference writes.
+struct StepInfo {
+    double mass = 0.0;      // compensated sum of the new interior density
+    double max_speed = 0.0; // max signal speed of the new state
+    unsigned err = 0;       // error bits of the launch
+    int kernel = 0;         // Kernel actually run
+};
+
+// One FVM step on the whole domain (periodic X by in-kernel wrap, reflective Y[/Z]).
+// Launches on `stream`, and when `sync` is true waits for it and fills *info.
+template <class T>
+int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
+           size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info);
+
+template <class T>
+int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
+           size_t nb_y, size_t nb_z, T DtDx, T DtDy, T DtDz, cudaStream_t stream, Kernel which, bool sync,
+           StepInfo *info);
+
+// Blast initial condition and first Dt on the device (hydro2d/main.cxx:280-338).
+template <class T>
+int init2d(T *rhoE, T *uv, size_t nb_x, size_t nb_y, T u_in, T u_out, T p_in, T p_out, T C_min, T gamma,
+           T *min_dt, cudaStream_t stream);
+template <class T>
+int init3d(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, T u_in, T u_out, T p_in, T p_out, T C_min,
+           T gamma, T *min_dt, cudaStream_t stream);
+
+// Compensated interior density sum on the device (hydro2d/main.cxx:237-265).
+template <class T> int mass_sum(const T *rhoE, size_t nb_x, size_t nb_y, size_t nb_z, double *out, cudaStream_t s);
+
+} // namespace hydro

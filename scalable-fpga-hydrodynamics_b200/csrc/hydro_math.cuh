@@ -1,0 +1,309 @@
+// Per-cell arithmetic of the first-order finite-volume update, device side.
+//
+// Every operation is an explicit round-to-nearest intrinsic (__dmul_rn, __dadd_rn,
+// __drcp_rn, __dsqrt_rn, and the float forms), so the compiler can neither contract a
+// multiply and an add into an FMA nor reassociate, whatever -fmad/-use_fast_math say.
+// Each expression keeps the association of the reference source it restates, which
+// makes the results bit-identical to the reference kernel compiled for an IEEE host
+// without contraction (x86-64 SSE2, -ffp-contract=off).
+//
+// Faces are computed once per face instead of once per adjacent cell as the reference
+// does (hydro2d/kernel.cxx:186-251 evaluates each face from both sides); the two
+// evaluations there take identical arguments, so one evaluation gives the same bits.
+// Quantities that depend on one cell only (primitives, the acoustic impedance
+// sqrt(gamma*p*rho), the upwinded conservative values) are computed once per cell.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hydro {
+
+template <class T> struct Ar;
+
+template <> struct Ar<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    // 1/x correctly rounded: the same value as ONE / x in IEEE double
+    static __device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double sqrt(double a) { return __dsqrt_rn(a); }
+    static constexpr double half = 0.5;
+};
+
+template <> struct Ar<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float rcp(float a) { return __frcp_rn(a); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    static __device__ __forceinline__ float sqrt(float a) { return __fsqrt_rn(a); }
+    static constexpr float half = 0.5f;
+};
+
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// std::max(a, b) as the reference calls it: a unless a < b
+template <class T> __device__ __forceinline__ T smax(T a, T b) { return (a < b) ? b : a; }
+
+// Physical constants of one launch (hydro2d/kernel.hpp:63-68 argument list).
+template <class T> struct Phys {
+    T C_min, gamma, gm1, divgamma, K;
+};
+
+// A cell seen by the face flux: everything compute_fluxes needs from one side
+// (hydro2d/kernel.cxx:74-118), with the normal velocity and normal/tangential momenta
+// already routed for the face direction.
+template <class T> struct FaceIn {
+    T r;   // density
+    T un;  // normal velocity
+    T p;   // pressure
+    T a;   // sqrt(gamma * p * rho)
+    T mn;  // un * rho   (the reference's U_upwind_ux for this direction)
+    T mt;  // ut * rho   (U_upwind_uy)
+    T eup; // p * divgamma + (0.5 * rho) * |u|^2   (U_upwind_p)
+};
+
+template <class T> struct FaceIn3 {
+    T r, un, p, a, mn, mt1, mt2, eup;
+};
+
+template <class T> struct Flux2 { T r, n, t, E; };
+template <class T> struct Flux3 { T r, n, t1, t2, E; };
+
+// Primitive variables of a 2D cell, hydro2d/kernel.cxx:5-29/31-53:
+//   inv = 1/rho ; u = rho_u*inv ; v = rho_v*inv ; temp = u*u + v*v
+//   p = (gm1*rho) * (E*inv - 0.5*temp)
+// plus the per-cell face quantities (a, u*rho, v*rho, upwinded energy).
+template <class T> struct Cell2 {
+    T r, u, v, p, a, mu, mv, eup;
+};
+
+template <class T>
+__device__ __forceinline__ Cell2<T> make_cell2(T ur, T uu, T uv, T uE, const Phys<T> &ph)
+{
+    using A = Ar<T>;
+    Cell2<T> c;
+    const T inv = A::rcp(ur);
+    c.r = ur;
+    c.u = A::mul(uu, inv);
+    c.v = A::mul(uv, inv);
+    const T temp = A::add(A::mul(c.u, c.u), A::mul(c.v, c.v));
+    const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
+    c.p = A::mul(A::mul(ph.gm1, ur), e_int);
+    // a_left = SQRT(gamma * Q_p_left * Q_rho_left)   (kernel.cxx:92)
+    c.a = A::sqrt(A::mul(A::mul(ph.gamma, c.p), c.r));
+    // U_upwind_ux/uy = Q_upwind_u * Q_upwind_rho      (kernel.cxx:109-110)
+    c.mu = A::mul(c.u, c.r);
+    c.mv = A::mul(c.v, c.r);
+    // U_upwind_p = Q_p*divgamma + (HALF*Q_rho)*(u*u + v*v)   (kernel.cxx:111); the sum
+    // of two squares commutes exactly, so x and y faces share one value.
+    c.eup = A::add(A::mul(c.p, ph.divgamma), A::mul(A::mul(A::half, c.r), temp));
+    return c;
+}
+
+// x faces: normal = u
+template <class T> __device__ __forceinline__ FaceIn<T> face_x(const Cell2<T> &c)
+{
+    return FaceIn<T>{c.r, c.u, c.p, c.a, c.mu, c.mv, c.eup};
+}
+// y faces: normal = v, the reference swaps (ux, uy) in the call (kernel.cxx:228-229)
+template <class T> __device__ __forceinline__ FaceIn<T> face_y(const Cell2<T> &c)
+{
+    return FaceIn<T>{c.r, c.v, c.p, c.a, c.mv, c.mu, c.eup};
+}
+// reflective wall: mirror state with the normal velocity negated (kernel.cxx:222-225);
+// -(v*rho) == (-v)*rho exactly, and the energy depends on v*v only.
+template <class T> __device__ __forceinline__ FaceIn<T> mirror(const FaceIn<T> &f)
+{
+    return FaceIn<T>{f.r, -f.un, f.p, f.a, -f.mn, f.mt, f.eup};
+}
+
+// compute_fluxes, hydro2d/kernel.cxx:74-118, from cached per-cell quantities.
+template <class T>
+__device__ __forceinline__ Flux2<T> face_flux(const FaceIn<T> &L, const FaceIn<T> &R, const Phys<T> &ph)
+{
+    using A = Ar<T>;
+    const T a = A::mul(ph.K, smax(L.a, R.a));
+    const T diva = A::rcp(a);
+    const T us = A::mul(A::half, A::sub(A::add(L.un, R.un), A::mul(diva, A::sub(R.p, L.p))));
+    const T ps = A::mul(A::half, A::sub(A::add(L.p, R.p), A::mul(a, A::sub(R.un, L.un))));
+    const bool up = us >= T(0);
+    const T r = up ? L.r : R.r;
+    const T mn = up ? L.mn : R.mn;
+    const T mt = up ? L.mt : R.mt;
+    const T e = up ? L.eup : R.eup;
+    Flux2<T> F;
+    F.r = A::add(A::mul(r, us), T(0)); // "+ ZERO" kept: it turns -0 into +0
+    F.n = A::add(A::mul(mn, us), ps);
+    F.t = A::add(A::mul(mt, us), T(0));
+    F.E = A::add(A::mul(e, us), A::mul(ps, us));
+    return F;
+}
+
+// The 2D conservative update and the new state's signal speed,
+// hydro2d/kernel.cxx:259-313. fx_lo/fx_hi are the faces at i-1/2 and i+1/2,
+// fy_lo/fy_hi at j-1/2 and j+1/2 (y fluxes carry the y momentum in .n).
+template <class T> struct Upd2 {
+    T r, u, v, E, speed;
+};
+
+template <class T>
+__device__ __forceinline__ Upd2<T> update2(T ur, T uu, T uv, T uE, const Flux2<T> &fx_lo, const Flux2<T> &fx_hi,
+                                           const Flux2<T> &fy_lo, const Flux2<T> &fy_hi, T DtDx, T DtDy,
+                                           const Phys<T> &ph)
+{
+    using A = Ar<T>;
+    const T x_r = A::mul(DtDx, A::sub(fx_lo.r, fx_hi.r));
+    const T x_u = A::mul(DtDx, A::sub(fx_lo.n, fx_hi.n));
+    const T x_v = A::mul(DtDx, A::sub(fx_lo.t, fx_hi.t));
+    const T x_E = A::mul(DtDx, A::sub(fx_lo.E, fx_hi.E));
+    const T y_r = A::mul(DtDy, A::sub(fy_lo.r, fy_hi.r));
+    const T y_u = A::mul(DtDy, A::sub(fy_lo.t, fy_hi.t));
+    const T y_v = A::mul(DtDy, A::sub(fy_lo.n, fy_hi.n));
+    const T y_E = A::mul(DtDy, A::sub(fy_lo.E, fy_hi.E));
+    Upd2<T> o;
+    o.r = A::add(A::add(ur, x_r), y_r);
+    o.u = A::add(A::add(uu, x_u), y_u);
+    o.v = A::add(A::add(uv, x_v), y_v);
+    o.E = A::add(A::add(uE, x_E), y_E);
+    const T inv = A::rcp(o.r);
+    const T qu = A::mul(o.u, inv);
+    const T qv = A::mul(o.v, inv);
+    const T temp = A::add(A::mul(qu, qu), A::mul(qv, qv));
+    const T e_int = A::sub(A::mul(o.E, inv), A::mul(A::half, temp));
+    const T p = A::mul(A::mul(ph.gm1, o.r), e_int);
+    const T c_s = A::sqrt(A::mul(A::mul(ph.gamma, p), inv));
+    const T Unorm = A::sqrt(temp);
+    o.speed = A::add(c_s, Unorm);
+    return o;
+}
+
+// ---------------------------------------------------------------- 3D ----------------
+// Primitive variables of a 3D cell, hydro3d/kernel.cxx:33-58:
+//   temp = (u*u + v*v) + w*w
+// The upwinded energy uses (un^2 + ut1^2) + ut2^2 with the per-direction order of the
+// reference's calls (hydro3d/kernel.cxx:121): x (u,v,w) and y (v,u,w) give the same sum
+// (the first addition commutes); z (w,v,u) is a different association, kept separately.
+template <class T> struct Cell3 {
+    T r, u, v, w, p, a, mu, mv, mw, eup_xy, eup_z;
+};
+
+template <class T>
+__device__ __forceinline__ Cell3<T> make_cell3(T ur, T uu, T uv, T uw, T uE, const Phys<T> &ph)
+{
+    using A = Ar<T>;
+    Cell3<T> c;
+    const T inv = A::rcp(ur);
+    c.r = ur;
+    c.u = A::mul(uu, inv);
+    c.v = A::mul(uv, inv);
+    c.w = A::mul(uw, inv);
+    const T uu2 = A::mul(c.u, c.u), vv2 = A::mul(c.v, c.v), ww2 = A::mul(c.w, c.w);
+    const T temp = A::add(A::add(uu2, vv2), ww2);
+    const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
+    c.p = A::mul(A::mul(ph.gm1, ur), e_int);
+    c.a = A::sqrt(A::mul(A::mul(ph.gamma, c.p), c.r));
+    c.mu = A::mul(c.u, c.r);
+    c.mv = A::mul(c.v, c.r);
+    c.mw = A::mul(c.w, c.r);
+    const T eint = A::mul(c.p, ph.divgamma);
+    const T hr = A::mul(A::half, c.r);
+    c.eup_xy = A::add(eint, A::mul(hr, temp));
+    c.eup_z = A::add(eint, A::mul(hr, A::add(A::add(ww2, vv2), uu2)));
+    return c;
+}
+
+// x faces: (u, v, w)
+template <class T> __device__ __forceinline__ FaceIn3<T> face3_x(const Cell3<T> &c)
+{
+    return FaceIn3<T>{c.r, c.u, c.p, c.a, c.mu, c.mv, c.mw, c.eup_xy};
+}
+// y faces: (v, u, w)   hydro3d/kernel.cxx:254-256
+template <class T> __device__ __forceinline__ FaceIn3<T> face3_y(const Cell3<T> &c)
+{
+    return FaceIn3<T>{c.r, c.v, c.p, c.a, c.mv, c.mu, c.mw, c.eup_xy};
+}
+// z faces: (w, v, u)   hydro3d/kernel.cxx:296-298
+template <class T> __device__ __forceinline__ FaceIn3<T> face3_z(const Cell3<T> &c)
+{
+    return FaceIn3<T>{c.r, c.w, c.p, c.a, c.mw, c.mv, c.mu, c.eup_z};
+}
+template <class T> __device__ __forceinline__ FaceIn3<T> mirror3(const FaceIn3<T> &f)
+{
+    return FaceIn3<T>{f.r, -f.un, f.p, f.a, -f.mn, f.mt1, f.mt2, f.eup};
+}
+
+// compute_fluxes, hydro3d/kernel.cxx:79-130
+template <class T>
+__device__ __forceinline__ Flux3<T> face_flux3(const FaceIn3<T> &L, const FaceIn3<T> &R, const Phys<T> &ph)
+{
+    using A = Ar<T>;
+    const T a = A::mul(ph.K, smax(L.a, R.a));
+    const T diva = A::rcp(a);
+    const T us = A::mul(A::half, A::sub(A::add(L.un, R.un), A::mul(diva, A::sub(R.p, L.p))));
+    const T ps = A::mul(A::half, A::sub(A::add(L.p, R.p), A::mul(a, A::sub(R.un, L.un))));
+    const bool up = us >= T(0);
+    const T r = up ? L.r : R.r;
+    const T mn = up ? L.mn : R.mn;
+    const T m1 = up ? L.mt1 : R.mt1;
+    const T m2 = up ? L.mt2 : R.mt2;
+    const T e = up ? L.eup : R.eup;
+    Flux3<T> F;
+    F.r = A::add(A::mul(r, us), T(0));
+    F.n = A::add(A::mul(mn, us), ps);
+    F.t1 = A::add(A::mul(m1, us), T(0));
+    F.t2 = A::add(A::mul(m2, us), T(0));
+    F.E = A::add(A::mul(e, us), A::mul(ps, us));
+    return F;
+}
+
+template <class T> struct Upd3 {
+    T r, u, v, w, E, speed;
+};
+
+// hydro3d/kernel.cxx:330-394. Slot routing per direction: x (n=u, t1=v, t2=w),
+// y (n=v, t1=u, t2=w), z (n=w, t1=v, t2=u).
+template <class T>
+__device__ __forceinline__ Upd3<T> update3(T ur, T uu, T uv, T uw, T uE, const Flux3<T> &fx_lo,
+                                           const Flux3<T> &fx_hi, const Flux3<T> &fy_lo, const Flux3<T> &fy_hi,
+                                           const Flux3<T> &fz_lo, const Flux3<T> &fz_hi, T DtDx, T DtDy, T DtDz,
+                                           const Phys<T> &ph)
+{
+    using A = Ar<T>;
+    const T x_r = A::mul(DtDx, A::sub(fx_lo.r, fx_hi.r));
+    const T x_u = A::mul(DtDx, A::sub(fx_lo.n, fx_hi.n));
+    const T x_v = A::mul(DtDx, A::sub(fx_lo.t1, fx_hi.t1));
+    const T x_w = A::mul(DtDx, A::sub(fx_lo.t2, fx_hi.t2));
+    const T x_E = A::mul(DtDx, A::sub(fx_lo.E, fx_hi.E));
+    const T y_r = A::mul(DtDy, A::sub(fy_lo.r, fy_hi.r));
+    const T y_u = A::mul(DtDy, A::sub(fy_lo.t1, fy_hi.t1));
+    const T y_v = A::mul(DtDy, A::sub(fy_lo.n, fy_hi.n));
+    const T y_w = A::mul(DtDy, A::sub(fy_lo.t2, fy_hi.t2));
+    const T y_E = A::mul(DtDy, A::sub(fy_lo.E, fy_hi.E));
+    const T z_r = A::mul(DtDz, A::sub(fz_lo.r, fz_hi.r));
+    const T z_u = A::mul(DtDz, A::sub(fz_lo.t2, fz_hi.t2));
+    const T z_v = A::mul(DtDz, A::sub(fz_lo.t1, fz_hi.t1));
+    const T z_w = A::mul(DtDz, A::sub(fz_lo.n, fz_hi.n));
+    const T z_E = A::mul(DtDz, A::sub(fz_lo.E, fz_hi.E));
+    Upd3<T> o;
+    o.r = A::add(A::add(A::add(ur, x_r), y_r), z_r);
+    o.u = A::add(A::add(A::add(uu, x_u), y_u), z_u);
+    o.v = A::add(A::add(A::add(uv, x_v), y_v), z_v);
+    o.w = A::add(A::add(A::add(uw, x_w), y_w), z_w);
+    o.E = A::add(A::add(A::add(uE, x_E), y_E), z_E);
+    const T inv = A::rcp(o.r);
+    const T qu = A::mul(o.u, inv), qv = A::mul(o.v, inv), qw = A::mul(o.w, inv);
+    const T temp = A::add(A::add(A::mul(qu, qu), A::mul(qv, qv)), A::mul(qw, qw));
+    const T e_int = A::sub(A::mul(o.E, inv), A::mul(A::half, temp));
+    const T p = A::mul(A::mul(ph.gm1, o.r), e_int);
+    const T c_s = A::sqrt(A::mul(A::mul(ph.gamma, p), inv));
+    const T Unorm = A::sqrt(temp);
+    o.speed = A::add(c_s, Unorm);
+    return o;
+}
+
+} // namespace hydro

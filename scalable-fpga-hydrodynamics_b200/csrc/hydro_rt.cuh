@@ -1,0 +1,245 @@
+// Device runtime pieces shared by the 2D and 3D kernels:
+//  - mbarrier / TMA (cp.async.bulk.tensor) inline-PTX wrappers, every wait bounded;
+//  - the fused end-of-step reduction: the CFL maximum signal speed (the reference
+//    folds it serially, hydro2d/kernel.cxx:313 and :318) and an FP64 compensated sum of
+//    the new density (the mass the reference sums on the host in long double,
+//    hydro2d/main.cxx:237-265), combined with warp shuffles, one partial per block and
+//    one ticket atomic per block; the last block to finish writes Dt_next and the
+//    status record and re-arms the scratch words for the next launch.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hydro_math.cuh"
+
+namespace hydro {
+
+// error bits reported in StepStatus::err and by hydro_last_error()
+enum : unsigned {
+    kErrNonPhysical = 1u,  // a new cell with rho <= 0 or a non-finite signal speed
+    kErrWaitTimeout = 2u,  // a bounded wait on a TMA barrier gave up
+};
+
+// Scratch words in device memory, one set per device context. max_bits and ticket
+// are zero between launches (the last block of each launch resets them).
+struct StepScratch {
+    unsigned long long max_bits; // max signal speed as the bits of a non-negative double
+    unsigned int ticket;         // blocks finished so far in this launch
+    unsigned int err;            // error bits raised in this launch
+    double pad[2];
+};
+
+// Result record of one launch, written by the last block (host-mapped memory).
+struct StepStatus {
+    double mass;      // sum of the new interior density (compensated FP64)
+    double mass_comp; // its compensation term
+    double max_speed; // max over interior cells of c_s + |u| of the new state
+    unsigned int err; // error bits
+    unsigned int seq; // launch sequence number, for the host to check completion
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of a barrier, giving up after ~2^31 clock cycles (about a
+// second). Returns false on time-out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > (1ll << 31)) return false;
+    }
+    return true;
+}
+
+// 2D tiled TMA load into shared memory, completion signalled on `bar`. The innermost
+// coordinate x must be a multiple of 16 bytes / element size (asserted by the host).
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int x, int y, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, int x, int y, int z, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tensormap(const CUtensorMap *tm)
+{
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tm)) : "memory");
+}
+
+// Neumaier-compensated accumulation (s, c) += x, the FP64 counterpart of the
+// reference's long-double loop (hydro2d/main.cxx:251-256).
+__device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
+{
+    const double t = __dadd_rn(s, x);
+    if (fabs(s) >= fabs(x)) c = __dadd_rn(c, __dadd_rn(__dsub_rn(s, t), x));
+    else c = __dadd_rn(c, __dadd_rn(__dsub_rn(x, t), s));
+    s = t;
+}
+
+__device__ __forceinline__ void neumaier_merge(double &s, double &c, double s2, double c2)
+{
+    neumaier_add(s, c, s2);
+    c = __dadd_rn(c, c2);
+}
+
+// Per-thread accumulator of the fused reductions.
+struct StepAcc {
+    double vmax = 0.0; // running max of the signal speed (NaN never enters: flagged instead)
+    double ms = 0.0, mc = 0.0;
+    unsigned err = 0;
+
+    template <class T> __device__ __forceinline__ void add_cell(T rho_new, T speed)
+    {
+        const double sp = static_cast<double>(speed);
+        vmax = (sp > vmax) ? sp : vmax;
+        if (!(rho_new > T(0)) || !(sp <= 1.0e300)) err |= kErrNonPhysical;
+        neumaier_add(ms, mc, static_cast<double>(rho_new));
+    }
+};
+
+// Block-wide combination of the accumulators, one partial per block, one ticket atomic
+// per block; the last block writes *Dt_next = C_min / max_speed (in T, as the
+// reference does at hydro2d/kernel.cxx:318) and the status record. NT = threads/block.
+template <int NT, class T>
+__device__ __forceinline__ void step_epilogue(StepAcc acc, StepScratch *scr, double2 *partials, unsigned nblocks,
+                                              unsigned bid, T C_min, T *Dt_next, StepStatus *status, unsigned seq)
+{
+    static_assert(NT % 32 == 0 && NT <= 1024, "block size");
+    constexpr int NW = NT / 32;
+    __shared__ unsigned long long s_max[NW];
+    __shared__ double s_ms[NW], s_mc[NW];
+    __shared__ unsigned s_err[NW];
+    __shared__ bool s_last;
+
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = t & 31, warp = t >> 5;
+    unsigned long long mb = __double_as_longlong(acc.vmax);
+    double ms = acc.ms, mc = acc.mc;
+    unsigned err = acc.err;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long om = __shfl_xor_sync(0xffffffffu, mb, o);
+        mb = om > mb ? om : mb;
+        const double s2 = __shfl_xor_sync(0xffffffffu, ms, o);
+        const double c2 = __shfl_xor_sync(0xffffffffu, mc, o);
+        if (lane & o) { // deterministic pairing: the higher lane folds into the lower
+            double a = s2, b = c2;
+            neumaier_merge(a, b, ms, mc);
+            ms = a; mc = b;
+        } else {
+            neumaier_merge(ms, mc, s2, c2);
+        }
+        err |= __shfl_xor_sync(0xffffffffu, err, o);
+    }
+    if (lane == 0) {
+        s_max[warp] = mb;
+        s_ms[warp] = ms;
+        s_mc[warp] = mc;
+        s_err[warp] = err;
+    }
+    __syncthreads();
+    if (t == 0) {
+        for (int w = 1; w < NW; ++w) {
+            mb = s_max[w] > mb ? s_max[w] : mb;
+            neumaier_merge(ms, mc, s_ms[w], s_mc[w]);
+            err |= s_err[w];
+        }
+        partials[bid] = make_double2(ms, mc);
+        atomicMax(&scr->max_bits, mb);
+        if (err) atomicOr(&scr->err, err);
+        __threadfence();
+        const unsigned prev = atomicAdd(&scr->ticket, 1u);
+        s_last = (prev == nblocks - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+
+    // last block: all partials and the max are visible after the fence
+    __threadfence();
+    double s = 0.0, c = 0.0;
+    for (unsigned b = t; b < nblocks; b += NT) {
+        const double2 p = __ldcg(&partials[b]);
+        neumaier_merge(s, c, p.x, p.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double s2 = __shfl_xor_sync(0xffffffffu, s, o);
+        const double c2 = __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane & o) {
+            double a = s2, b = c2;
+            neumaier_merge(a, b, s, c);
+            s = a; c = b;
+        } else {
+            neumaier_merge(s, c, s2, c2);
+        }
+    }
+    if (lane == 0) {
+        s_ms[warp] = s;
+        s_mc[warp] = c;
+    }
+    __syncthreads();
+    if (t == 0) {
+        for (int w = 1; w < NW; ++w) neumaier_merge(s, c, s_ms[w], s_mc[w]);
+        const unsigned long long gm = atomicAdd(&scr->max_bits, 0ull);
+        const unsigned gerr = atomicAdd(&scr->err, 0u);
+        const double vmax = __longlong_as_double(static_cast<long long>(gm));
+        // the max of values of type T, held exactly in a double, converts back exactly
+        *Dt_next = Ar<T>::div(C_min, static_cast<T>(vmax));
+        if (status) {
+            status->mass = s;
+            status->mass_comp = c;
+            status->max_speed = vmax;
+            status->err = gerr;
+            __threadfence_system();
+            status->seq = seq;
+        }
+        scr->max_bits = 0ull;
+        scr->err = 0u;
+        __threadfence();
+        scr->ticket = 0u;
+    }
+}
+
+} // namespace hydro
