@@ -202,6 +202,26 @@ def host_loop(stepper, init_state, phys, first_dt, max_t, max_it):
     return cur, t_log, dt_log
 
 
+def interior(st, nb):
+    """The interior cells of a state tuple as (rhoE, uvx) arrays of shape nb + (nv,).
+    Ghost cells are excluded: the reference host writes the X ghosts of its copy, the
+    device kernels never read or write them."""
+    nv = 3 if len(nb) == 3 else 2
+    shape = tuple(n + 2 for n in nb)
+    inner = tuple(slice(1, n + 1) for n in nb)
+    return (st[0].reshape(shape + (2,))[inner], st[1].reshape(shape + (nv,))[inner])
+
+
+def interior_digest(st, nb):
+    """SHA-256 of the interior cells' bytes (rhoE then uvx, row-major)."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for a in interior(st, nb):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
 def ghost_x_numpy(st, nb):
     """Periodic X ghost rows/planes by copy (hydro2d/main.cxx:349-378)."""
     plane = int(np.prod([n + 2 for n in nb[1:]]))

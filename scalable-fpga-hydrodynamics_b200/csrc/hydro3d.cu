@@ -344,11 +344,10 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
         g.partials = ctx->partials;
         const int smem = (int)sizeof(Smem3<T>);
-        static bool attr_set[2] = {false, false};
-        bool &done = attr_set[sizeof(T) == 8];
-        if (!done) {
-            cudaFuncSetAttribute(strip3d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            done = true;
+        cudaError_t ea = cudaFuncSetAttribute(strip3d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (ea != cudaSuccess) {
+            set_error(kErrCuda, "step3d: shared-memory attribute: %s", cudaGetErrorString(ea));
+            return kErrCuda;
         }
         strip3d<T><<<dim3(nz, ny, nchunks), k3NT, smem, stream>>>(g);
     } else {

@@ -113,7 +113,7 @@ def ref_runs():
         ref = orc.RefKernel(len(nb), T)
         fin, t_log, dt_log = orc.host_loop(ref.step, st, phys, first, max_t, max_it)
         meta[name] = dict(nb=list(nb), dtype=np.dtype(T).name, max_t=max_t, max_it=max_it, it=len(t_log),
-                          first_dt=float(first), sha256=digest(fin), mass1=o.mass(fin[0], nb))
+                          first_dt=float(first), sha256=orc.interior_digest(fin, nb), mass1=o.mass(fin[0], nb))
         arrays[name + "__t"] = np.array(t_log, np.float64)
         arrays[name + "__dt"] = np.array(dt_log, T)
         if whole:

@@ -32,6 +32,11 @@ def seeded_state(nb, T, seed):
     return rhoE, uvx
 
 
+def cfl_dt(phys, seed):
+    """A stable time step for seeded_state (signal speeds below ~6): CFL 0.05-0.1."""
+    return phys.dtype(0.05 * (1 + seed % 2)) * phys.min_spacing / phys.dtype(6)
+
+
 SHAPES_2D = [(1, 1), (1, 9), (9, 1), (2, 3), (7, 5), (33, 17), (60, 60), (5, 130), (3, 257)]
 SHAPES_3D = [(1, 1, 1), (1, 3, 4), (4, 1, 3), (3, 4, 1), (5, 6, 7), (12, 10, 9), (3, 2, 33)]
 
@@ -47,7 +52,7 @@ def test_oracle_step_matches_reference_kernel(oracle, orc, nb, T):
         st = seeded_state(nb, T, seed)
         a = (np.zeros_like(st[0]), np.zeros_like(st[1]))
         b = (np.zeros_like(st[0]), np.zeros_like(st[1]))
-        dtd = phys.dtd(T(1e-3) * T(seed + 1))
+        dtd = phys.dtd(cfl_dt(phys, seed))
         d1 = oracle.step(st, a, phys, dtd)
         d2 = ref.step(st, b, phys, dtd)
         assert d1.tobytes() == d2.tobytes()
@@ -82,7 +87,7 @@ def digest(state):
     return h.hexdigest()
 
 
-def test_oracle_matches_golden_runs(oracle, ref_runs):
+def test_oracle_matches_golden_runs(oracle, orc, ref_runs):
     meta, arrays = ref_runs
     for name, m in meta.items():
         if np.prod(m["nb"]) > 100_000:
@@ -92,7 +97,7 @@ def test_oracle_matches_golden_runs(oracle, ref_runs):
         assert r["it"] == m["it"], name
         assert np.array_equal(r["t"], arrays[name + "__t"]), name
         assert np.array_equal(r["dt"], arrays[name + "__dt"]), name
-        assert digest(r["state"]) == m["sha256"], name
+        assert orc.interior_digest(r["state"], tuple(m["nb"])) == m["sha256"], name
         assert float(r["first_dt"]) == m["first_dt"], name
 
 
