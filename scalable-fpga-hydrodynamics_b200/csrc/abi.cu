@@ -46,7 +46,10 @@ double finish_launcher(int rc, double t0, const char *what)
     return -1.0;
 }
 
-template <class T> Phys<T> phys(T C_min, T gamma, T gm1, T divgamma, T K) { return Phys<T>{C_min, gamma, gm1, divgamma, K}; }
+template <class T> Phys<T> phys(T C_min, T gamma, T gm1, T divgamma, T K)
+{
+    return Phys<T>{C_min, gamma, gm1, divgamma, K, K < T(0)};
+}
 
 void fill(hydro_step_info_t *out, const StepInfo &in)
 {

@@ -43,7 +43,16 @@ template <class T> struct Args2 {
     double2 *partials;
     StepStatus *status;
     unsigned seq;
+    unsigned long long key; // problem key for the signal-speed skip (0: never skip)
+    float ggm1;             // gamma * (gamma - 1), for the speed upper bound
 };
+
+// The float skip threshold, rounded down so that every skipped cell is provably below
+// the double threshold the last block checks against.
+__device__ __forceinline__ float skip_threshold_f(const StepScratch *scr, unsigned long long key)
+{
+    return __double2float_rd(skip_threshold(scr, key));
+}
 
 __device__ __forceinline__ int wrap_row(int n, int nb_x) { return n == 0 ? nb_x : (n == nb_x + 1 ? 1 : n); }
 
@@ -86,10 +95,25 @@ template <class T> __global__ void __launch_bounds__(kDirectNT) direct2d(Args2<T
         g.rhoE_n[2 * c + 1] = o.E;
         g.uv_n[2 * c] = o.u;
         g.uv_n[2 * c + 1] = o.v;
-        acc.add_cell(o.r, o.speed);
+        acc.add_cell(o.r, speed2(o.r, o.u, o.v, o.E, g.ph));
     }
     step_epilogue<kDirectNT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y, blockIdx.x + blockIdx.y * gridDim.x,
-                                g.ph.C_min, g.Dt_next, g.status, g.seq);
+                                g.ph.C_min, g.Dt_next, g.status, g.seq, 0.0, g.key);
+}
+
+// Redo pass: the exact signal speed of every interior cell of the new state, when the
+// step's skip threshold turned out too high (StepScratch::redo); exits at once otherwise.
+constexpr int kRedoNT = 256;
+template <class T> __global__ void __launch_bounds__(kRedoNT) redo2d(Args2<T> g)
+{
+    if (*reinterpret_cast<const volatile unsigned *>(&g.scr->redo) == 0u) return;
+    StepAcc acc;
+    const long long n = (long long)g.nb_x * g.nb_y;
+    for (long long q = blockIdx.x * (long long)kRedoNT + threadIdx.x; q < n; q += (long long)gridDim.x * kRedoNT) {
+        const long long c = (1 + q / g.nb_y) * g.ys + 1 + q % g.nb_y;
+        acc.add_speed(speed2(g.rhoE_n[2 * c], g.uv_n[2 * c], g.uv_n[2 * c + 1], g.rhoE_n[2 * c + 1], g.ph));
+    }
+    redo_epilogue<kRedoNT, T>(acc.vmax, acc.err, g.scr, gridDim.x, g.ph.C_min, g.Dt_next, g.status, g.key);
 }
 
 // ------------------------------------------------------------------- strip kernel ---
@@ -98,7 +122,7 @@ constexpr int kStripW = kStripNT - 2; // interior columns per strip
 constexpr int kStages = 4;
 
 template <class T>
-__global__ void __launch_bounds__(kStripNT, 3)
+__global__ void __launch_bounds__(kStripNT, 4)
     strip2d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args2<T> g)
 {
     using V2 = typename Vec2<T>::type;
@@ -107,11 +131,14 @@ __global__ void __launch_bounds__(kStripNT, 3)
     __shared__ __align__(128) V2 sr[kStages][kStripNT];
     __shared__ __align__(128) V2 su[kStages][kStripNT];
     __shared__ __align__(8) uint64_t full[kStages];
-    __shared__ T xP[kStripNT / 32][7];
-    __shared__ T xF[kStripNT / 32][4];
+    // y-face inputs of every lane's cell (lane t at [t]) and every lane's right face flux
+    // (lane t at [t+1]), stored as pairs so that each lane moves them with 128-bit
+    // (FP64) / 64-bit (FP32) shared-memory accesses
+    __shared__ __align__(16) V2 xP[4][kStripNT + 1];
+    __shared__ __align__(16) V2 xF[2][kStripNT + 1];
     __shared__ int s_abort;
 
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int t = threadIdx.x;
     const int jbase = kStripW * blockIdx.x; // column held by lane 0
     const int j = jbase + t;
     const int i0 = 1 + g.chunk * blockIdx.y;
@@ -119,6 +146,8 @@ __global__ void __launch_bounds__(kStripNT, 3)
     const int nrows = i1 - i0 + 3; // with one halo row above and below
     const bool interior = (t >= 1) && (t <= kStripW) && (j <= g.nb_y);
     const int xcoord = 2 * jbase;
+    // the two wall faces live in at most two warps; the others skip the mirror selects
+    const bool wall_warp = __any_sync(FULL, j == 0 || j == g.nb_y);
 
     if (t == 0) {
         prefetch_tensormap(&tmr);
@@ -142,64 +171,65 @@ __global__ void __launch_bounds__(kStripNT, 3)
     Cell2<T> Pm{};
     T Ur = 0, Uu = 0, Uv = 0, UE = 0;
     Flux2<T> fxlo{}, fyl{}, fyr{};
+    // lanes whose column is a ghost (j = 0, j = NB_Y+1) or past the array hold zeros;
+    // their primitives are never used, so they convert a unit state instead (keeps the
+    // reciprocal / square root of every lane on its regular path)
+    const bool real_col = (j >= 1) && (j <= g.nb_y);
+    const float tlof = skip_threshold_f(g.scr, g.key);
     int m = 0;
+#pragma unroll 2
     for (; m < nrows; ++m) {
         const int s = m % kStages;
         if (!mbar_wait_bounded(&full[s], (m / kStages) & 1)) s_abort = 1;
-        const V2 a = sr[s][t], b = su[s][t];
+        V2 a = sr[s][t], b = su[s][t];
+        if (!real_col) {
+            a = mk2<T>(T(1), T(1));
+            b = mk2<T>(T(0), T(0));
+        }
         const Cell2<T> P = make_cell2<T>(a.x, b.x, b.y, a.y, g.ph);
         const bool yrow = (m >= 1) && (m <= nrows - 2);
-        if (yrow && lane == 0) {
-            T *x = xP[warp];
-            x[0] = P.r; x[1] = P.v; x[2] = P.p; x[3] = P.a; x[4] = P.mv; x[5] = P.mu; x[6] = P.eup;
+        if (yrow) {
+            const FaceIn<T> me = face_y(P);
+            xP[0][t] = mk2<T>(me.r, me.un);
+            xP[1][t] = mk2<T>(me.p, me.Ka);
+            xP[2][t] = mk2<T>(me.iKa, me.mn);
+            xP[3][t] = mk2<T>(me.mt, me.eup);
         }
-        __syncthreads(); // stage s consumed by every lane; warp-edge primitives published
+        __syncthreads(); // stage s consumed by every lane; y-face inputs published
         if (s_abort) break;
         if (t == 0 && m + kStages < nrows) issue(m + kStages);
 
         if (m >= 1) {
+            // x face (row n-1 | row n) of this column; then the update of row n-1
             const Flux2<T> fxhi = face_flux(face_x(Pm), face_x(P), g.ph);
             if (m >= 2 && interior) {
                 const Upd2<T> o = update2(Ur, Uu, Uv, UE, fxlo, fxhi, fyl, fyr, g.DtDx, g.DtDy, g.ph);
                 const long long c = (long long)(i0 + m - 2) * g.ys + j;
                 reinterpret_cast<V2 *>(g.rhoE_n)[c] = mk2<T>(o.r, o.E);
                 reinterpret_cast<V2 *>(g.uv_n)[c] = mk2<T>(o.u, o.v);
-                acc.add_cell(o.r, o.speed);
+                acc.add_mass(o.r);
+                const float fu = (float)o.u, fv = (float)o.v;
+                const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv, g.ggm1);
+                if (!(ub < tlof)) acc.add_speed(speed2(o.r, o.u, o.v, o.E, g.ph));
             }
             fxlo = fxhi;
         }
         if (yrow) {
+            // y face (j | j+1) of row n, from this lane's cell and the next lane's
             const FaceIn<T> me = face_y(P);
-            FaceIn<T> nb;
-            nb.r = __shfl_down_sync(FULL, me.r, 1);
-            nb.un = __shfl_down_sync(FULL, me.un, 1);
-            nb.p = __shfl_down_sync(FULL, me.p, 1);
-            nb.a = __shfl_down_sync(FULL, me.a, 1);
-            nb.mn = __shfl_down_sync(FULL, me.mn, 1);
-            nb.mt = __shfl_down_sync(FULL, me.mt, 1);
-            nb.eup = __shfl_down_sync(FULL, me.eup, 1);
-            if (lane == 31 && warp + 1 < kStripNT / 32) {
-                const T *x = xP[warp + 1];
-                nb = FaceIn<T>{x[0], x[1], x[2], x[3], x[4], x[5], x[6]};
+            const V2 n0 = xP[0][t + 1], n1 = xP[1][t + 1], n2 = xP[2][t + 1], n3 = xP[3][t + 1];
+            FaceIn<T> L = me;
+            FaceIn<T> R{n0.x, n0.y, n1.x, n1.y, n2.x, n2.y, n3.x, n3.y};
+            if (wall_warp) {
+                if (j == 0) L = mirror(R);       // wall at j = 1/2
+                if (j == g.nb_y) R = mirror(me); // wall at j = NB_Y + 1/2
             }
-            FaceIn<T> L = me, R = nb;
-            if (j == 0) L = mirror(nb);        // wall at j = 1/2
-            if (j == g.nb_y) R = mirror(me);   // wall at j = NB_Y + 1/2
-            const Flux2<T> f = face_flux(L, R, g.ph);
-            if (lane == 31) {
-                T *x = xF[warp];
-                x[0] = f.r; x[1] = f.n; x[2] = f.t; x[3] = f.E;
-            }
-            __syncthreads(); // warp-edge face fluxes published
-            fyr = f;
-            fyl.r = __shfl_up_sync(FULL, f.r, 1);
-            fyl.n = __shfl_up_sync(FULL, f.n, 1);
-            fyl.t = __shfl_up_sync(FULL, f.t, 1);
-            fyl.E = __shfl_up_sync(FULL, f.E, 1);
-            if (lane == 0 && warp > 0) {
-                const T *x = xF[warp - 1];
-                fyl = Flux2<T>{x[0], x[1], x[2], x[3]};
-            }
+            fyr = face_flux(L, R, g.ph);
+            xF[0][t + 1] = mk2<T>(fyr.r, fyr.n);
+            xF[1][t + 1] = mk2<T>(fyr.t, fyr.E);
+            __syncthreads(); // right faces published: lane t's left face is lane t-1's right
+            const V2 f0 = xF[0][t], f1 = xF[1][t];
+            fyl = Flux2<T>{f0.x, f0.y, f1.x, f1.y};
         }
         Pm = P;
         Ur = a.x; Uu = b.x; Uv = b.y; UE = a.y;
@@ -214,7 +244,7 @@ __global__ void __launch_bounds__(kStripNT, 3)
         __syncthreads();
     }
     step_epilogue<kStripNT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y, blockIdx.x + blockIdx.y * gridDim.x,
-                               g.ph.C_min, g.Dt_next, g.status, g.seq);
+                               g.ph.C_min, g.Dt_next, g.status, g.seq, (double)tlof, g.key);
 }
 
 // ------------------------------------------------------------- initial condition ---
@@ -357,6 +387,8 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
     g.ph = ph; g.DtDx = DtDx; g.DtDy = DtDy;
     g.nb_x = (int)nb_x; g.nb_y = (int)nb_y; g.ys = (long long)nb_y + 2;
     g.scr = ctx->scr; g.status = ctx->status_d; g.seq = ++ctx->seq;
+    g.key = problem_key(Dt_next, nb_x, nb_y, 0, sizeof(T), ph);
+    g.ggm1 = (float)ph.gamma * (float)ph.gm1;
 
     using V2 = typename Vec2<T>::type;
     const size_t rowbytes = 2 * sizeof(T) * (nb_y + 2);
@@ -407,11 +439,25 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
         return kErrCuda;
     }
     ctx->last_kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
+    const unsigned redo_blocks = 148 * 4;
     if (!sync) {
+        // enqueued unconditionally; returns at once unless the step asked for it
+        redo2d<T><<<redo_blocks, kRedoNT, 0, stream>>>(g);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            ctx->dirty = true;
+            set_error(kErrCuda, "step2d launch: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
         if (info) info->kernel = ctx->last_kernel;
         return kOk;
     }
     e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && read_status(ctx->status_h).redo) {
+        redo2d<T><<<redo_blocks, kRedoNT, 0, stream>>>(g);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    }
     if (e != cudaSuccess) {
         ctx->dirty = true;
         set_error(kErrCuda, "step2d: %s", cudaGetErrorString(e));

@@ -37,6 +37,8 @@ template <class T> struct Args3 {
     double2 *partials;
     StepStatus *status;
     unsigned seq;
+    unsigned long long key; // problem key for the signal-speed skip (0: never skip)
+    float ggm1;             // gamma * (gamma - 1), for the speed upper bound
 };
 
 __device__ __forceinline__ int wrap_plane(int n, int nb_x) { return n == 0 ? nb_x : (n == nb_x + 1 ? 1 : n); }
@@ -78,11 +80,28 @@ template <class T> __global__ void __launch_bounds__(128) direct3d(Args3<T> g)
         g.uvw_n[3 * c] = o.u;
         g.uvw_n[3 * c + 1] = o.v;
         g.uvw_n[3 * c + 2] = o.w;
-        acc.add_cell(o.r, o.speed);
+        acc.add_cell(o.r, speed3(o.r, o.u, o.v, o.w, o.E, g.ph));
     }
     step_epilogue<128, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
                           blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
-                          g.status, g.seq);
+                          g.status, g.seq, 0.0, g.key);
+}
+
+// Redo pass (see StepScratch): the exact signal speed of every interior cell.
+constexpr int k3RedoNT = 256;
+template <class T> __global__ void __launch_bounds__(k3RedoNT) redo3d(Args3<T> g)
+{
+    if (*reinterpret_cast<const volatile unsigned *>(&g.scr->redo) == 0u) return;
+    StepAcc acc;
+    const long long ncol = (long long)g.nb_y * g.nb_z;
+    const long long n = (long long)g.nb_x * ncol;
+    for (long long q = blockIdx.x * (long long)k3RedoNT + threadIdx.x; q < n; q += (long long)gridDim.x * k3RedoNT) {
+        const long long r = q % ncol;
+        const long long c = (1 + q / ncol) * g.zy + (1 + r / g.nb_z) * g.zs + 1 + r % g.nb_z;
+        acc.add_speed(speed3(g.rhoE_n[2 * c], g.uvw_n[3 * c], g.uvw_n[3 * c + 1], g.uvw_n[3 * c + 2],
+                             g.rhoE_n[2 * c + 1], g.ph));
+    }
+    redo_epilogue<k3RedoNT, T>(acc.vmax, acc.err, g.scr, gridDim.x, g.ph.C_min, g.Dt_next, g.status, g.key);
 }
 
 // ------------------------------------------------------------------- strip kernel ---
@@ -108,7 +127,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile(
 
 template <class T> struct Smem3 {
     T st[k3Stages][5][k3NT];      // per plane: rho, E, rho_u, rho_v, rho_w
-    T xP[2][8][k3NT];             // y-face inputs of each lane's cell, by plane parity
+    T xP[2][9][k3NT];             // y-face inputs of each lane's cell, by plane parity
     T xF[2][5][k3NT];             // each lane's +y face flux, by plane parity
 };
 
@@ -150,6 +169,7 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
     Cell3<T> Pm{};
     T Ur = 0, Uu = 0, Uv = 0, Uw = 0, UE = 0;
     Flux3<T> fxlo{};
+    const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
     for (int m = 0; m < nplanes; ++m) {
         issue(m + k3Stages - 1);
         cp_async_wait<k3Stages - 1>();
@@ -160,8 +180,9 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
         {
             const FaceIn3<T> fy = face3_y(P);
             T *x = &S.xP[m & 1][0][t];
-            x[0 * k3NT] = fy.r; x[1 * k3NT] = fy.un; x[2 * k3NT] = fy.p; x[3 * k3NT] = fy.a;
-            x[4 * k3NT] = fy.mn; x[5 * k3NT] = fy.mt1; x[6 * k3NT] = fy.mt2; x[7 * k3NT] = fy.eup;
+            x[0 * k3NT] = fy.r; x[1 * k3NT] = fy.un; x[2 * k3NT] = fy.p; x[3 * k3NT] = fy.Ka;
+            x[4 * k3NT] = fy.iKa; x[5 * k3NT] = fy.mn; x[6 * k3NT] = fy.mt1; x[7 * k3NT] = fy.mt2;
+            x[8 * k3NT] = fy.eup;
         }
         Flux3<T> fxhi{};
         if (m >= 1 && iwarp) fxhi = face_flux3(face3_x(Pm), face3_x(P), g.ph);
@@ -173,8 +194,8 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
             Flux3<T> fy{};
             if (w < k3Warps - 1) {
                 const T *x = &S.xP[(m - 1) & 1][0][t + 32];
-                FaceIn3<T> nb{x[0 * k3NT], x[1 * k3NT], x[2 * k3NT], x[3 * k3NT],
-                              x[4 * k3NT], x[5 * k3NT], x[6 * k3NT], x[7 * k3NT]};
+                FaceIn3<T> nb{x[0 * k3NT], x[1 * k3NT], x[2 * k3NT], x[3 * k3NT], x[4 * k3NT],
+                              x[5 * k3NT], x[6 * k3NT], x[7 * k3NT], x[8 * k3NT]};
                 FaceIn3<T> L = me, R = nb;
                 if (j == 0) L = mirror3(nb);
                 if (j == g.nb_y) R = mirror3(me);
@@ -191,7 +212,8 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
                 nz.r = __shfl_down_sync(FULL, mz.r, 1);
                 nz.un = __shfl_down_sync(FULL, mz.un, 1);
                 nz.p = __shfl_down_sync(FULL, mz.p, 1);
-                nz.a = __shfl_down_sync(FULL, mz.a, 1);
+                nz.Ka = __shfl_down_sync(FULL, mz.Ka, 1);
+                nz.iKa = __shfl_down_sync(FULL, mz.iKa, 1);
                 nz.mn = __shfl_down_sync(FULL, mz.mn, 1);
                 nz.mt1 = __shfl_down_sync(FULL, mz.mt1, 1);
                 nz.mt2 = __shfl_down_sync(FULL, mz.mt2, 1);
@@ -220,7 +242,10 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
                     g.uvw_n[3 * c] = o.u;
                     g.uvw_n[3 * c + 1] = o.v;
                     g.uvw_n[3 * c + 2] = o.w;
-                    acc.add_cell(o.r, o.speed);
+                    acc.add_mass(o.r);
+                    const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
+                    const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, g.ggm1);
+                    if (!(ub < tlof)) acc.add_speed(speed3(o.r, o.u, o.v, o.w, o.E, g.ph));
                 }
             }
         } else {
@@ -233,7 +258,7 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
     cp_async_wait<0>();
     step_epilogue<k3NT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
                            blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
-                           g.status, g.seq);
+                           g.status, g.seq, (double)tlof, g.key);
 }
 
 // ------------------------------------------------------------- initial condition ---
@@ -321,6 +346,8 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
     g.nb_x = (int)nb_x; g.nb_y = (int)nb_y; g.nb_z = (int)nb_z;
     g.zs = (long long)nb_z + 2; g.zy = (long long)(nb_y + 2) * g.zs;
     g.scr = ctx->scr; g.status = ctx->status_d; g.seq = ++ctx->seq;
+    g.key = problem_key(Dt_next, nb_x, nb_y, nb_z, sizeof(T), ph);
+    g.ggm1 = (float)ph.gamma * (float)ph.gm1;
 
     const bool use_strip = which != Kernel::Direct;
     unsigned nblocks;
@@ -369,11 +396,25 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         return kErrCuda;
     }
     ctx->last_kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
+    const unsigned redo_blocks = 148 * 4;
     if (!sync) {
+        // enqueued unconditionally; returns at once unless the step asked for it
+        redo3d<T><<<redo_blocks, k3RedoNT, 0, stream>>>(g);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            ctx->dirty = true;
+            set_error(kErrCuda, "step3d launch: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
         if (info) info->kernel = ctx->last_kernel;
         return kOk;
     }
     e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && read_status(ctx->status_h).redo) {
+        redo3d<T><<<redo_blocks, k3RedoNT, 0, stream>>>(g);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    }
     if (e != cudaSuccess) {
         ctx->dirty = true;
         set_error(kErrCuda, "step3d: %s", cudaGetErrorString(e));

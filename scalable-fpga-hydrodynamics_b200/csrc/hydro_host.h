@@ -41,6 +41,8 @@ inline StepStatus read_status(const StepStatus *p)
     s.max_speed = v->max_speed;
     s.err = v->err;
     s.seq = v->seq;
+    s.redo = v->redo;
+    s.pad = 0;
     return s;
 }
 
@@ -49,6 +51,21 @@ template <class T> inline T div_zero(T a)
 {
     volatile T z = T(0);
     return a / z;
+}
+
+// Key of a problem for the signal-speed skip history: the Dt_next address, the grid and
+// the precision. 0 (never skip) when the speed bound's premise gamma > 1 fails.
+template <class T>
+inline unsigned long long problem_key(const void *dt_next, size_t a, size_t b, size_t c, size_t tsize,
+                                      const Phys<T> &ph)
+{
+    if (!(ph.gamma > T(1))) return 0ull;
+    unsigned long long k = reinterpret_cast<uintptr_t>(dt_next);
+    k ^= (a + 0x9E3779B97F4A7C15ull) * 0xBF58476D1CE4E5B9ull;
+    k ^= (b + 0x632BE59BD9B4E019ull) * 0x94D049BB133111EBull;
+    k ^= (c + 0x2545F4914F6CDD1Dull) * 0xD6E8FEB86659FD93ull;
+    k ^= tsize << 56;
+    return k ? k : 1ull;
 }
 
 // Context of the current device (created on first use; never freed before exit).

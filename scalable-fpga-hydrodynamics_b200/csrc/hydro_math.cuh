@@ -52,23 +52,31 @@ template <class T> __device__ __forceinline__ T smax(T a, T b) { return (a < b) 
 // Physical constants of one launch (hydro2d/kernel.hpp:63-68 argument list).
 template <class T> struct Phys {
     T C_min, gamma, gm1, divgamma, K;
+    bool kneg; // K < 0
 };
 
 // A cell seen by the face flux: everything compute_fluxes needs from one side
 // (hydro2d/kernel.cxx:74-118), with the normal velocity and normal/tangential momenta
 // already routed for the face direction.
+//
+// The face's acoustic impedance a = K * max(a_left, a_right) (kernel.cxx:95) is always
+// one of the two per-cell products K*a_left, K*a_right (the same rounded product), and
+// 1/a (kernel.cxx:97) is then one of the two per-cell reciprocals. Both are computed
+// once per cell and the face only selects: a monotone rounding keeps the choice
+// identical to comparing the unscaled a's (equal products are the same value).
 template <class T> struct FaceIn {
     T r;   // density
     T un;  // normal velocity
     T p;   // pressure
-    T a;   // sqrt(gamma * p * rho)
+    T Ka;  // K * sqrt(gamma * p * rho)
+    T iKa; // 1 / (K * sqrt(gamma * p * rho))
     T mn;  // un * rho   (the reference's U_upwind_ux for this direction)
     T mt;  // ut * rho   (U_upwind_uy)
     T eup; // p * divgamma + (0.5 * rho) * |u|^2   (U_upwind_p)
 };
 
 template <class T> struct FaceIn3 {
-    T r, un, p, a, mn, mt1, mt2, eup;
+    T r, un, p, Ka, iKa, mn, mt1, mt2, eup;
 };
 
 template <class T> struct Flux2 { T r, n, t, E; };
@@ -79,7 +87,7 @@ template <class T> struct Flux3 { T r, n, t1, t2, E; };
 //   p = (gm1*rho) * (E*inv - 0.5*temp)
 // plus the per-cell face quantities (a, u*rho, v*rho, upwinded energy).
 template <class T> struct Cell2 {
-    T r, u, v, p, a, mu, mv, eup;
+    T r, u, v, p, Ka, iKa, mu, mv, eup;
 };
 
 template <class T>
@@ -94,8 +102,9 @@ __device__ __forceinline__ Cell2<T> make_cell2(T ur, T uu, T uv, T uE, const Phy
     const T temp = A::add(A::mul(c.u, c.u), A::mul(c.v, c.v));
     const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
     c.p = A::mul(A::mul(ph.gm1, ur), e_int);
-    // a_left = SQRT(gamma * Q_p_left * Q_rho_left)   (kernel.cxx:92)
-    c.a = A::sqrt(A::mul(A::mul(ph.gamma, c.p), c.r));
+    // a_left = SQRT(gamma * Q_p_left * Q_rho_left)   (kernel.cxx:92), scaled by K
+    c.Ka = A::mul(ph.K, A::sqrt(A::mul(A::mul(ph.gamma, c.p), c.r)));
+    c.iKa = A::rcp(c.Ka);
     // U_upwind_ux/uy = Q_upwind_u * Q_upwind_rho      (kernel.cxx:109-110)
     c.mu = A::mul(c.u, c.r);
     c.mv = A::mul(c.v, c.r);
@@ -108,18 +117,18 @@ __device__ __forceinline__ Cell2<T> make_cell2(T ur, T uu, T uv, T uE, const Phy
 // x faces: normal = u
 template <class T> __device__ __forceinline__ FaceIn<T> face_x(const Cell2<T> &c)
 {
-    return FaceIn<T>{c.r, c.u, c.p, c.a, c.mu, c.mv, c.eup};
+    return FaceIn<T>{c.r, c.u, c.p, c.Ka, c.iKa, c.mu, c.mv, c.eup};
 }
 // y faces: normal = v, the reference swaps (ux, uy) in the call (kernel.cxx:228-229)
 template <class T> __device__ __forceinline__ FaceIn<T> face_y(const Cell2<T> &c)
 {
-    return FaceIn<T>{c.r, c.v, c.p, c.a, c.mv, c.mu, c.eup};
+    return FaceIn<T>{c.r, c.v, c.p, c.Ka, c.iKa, c.mv, c.mu, c.eup};
 }
 // reflective wall: mirror state with the normal velocity negated (kernel.cxx:222-225);
 // -(v*rho) == (-v)*rho exactly, and the energy depends on v*v only.
 template <class T> __device__ __forceinline__ FaceIn<T> mirror(const FaceIn<T> &f)
 {
-    return FaceIn<T>{f.r, -f.un, f.p, f.a, -f.mn, f.mt, f.eup};
+    return FaceIn<T>{f.r, -f.un, f.p, f.Ka, f.iKa, -f.mn, f.mt, f.eup};
 }
 
 // compute_fluxes, hydro2d/kernel.cxx:74-118, from cached per-cell quantities.
@@ -127,8 +136,11 @@ template <class T>
 __device__ __forceinline__ Flux2<T> face_flux(const FaceIn<T> &L, const FaceIn<T> &R, const Phys<T> &ph)
 {
     using A = Ar<T>;
-    const T a = A::mul(ph.K, smax(L.a, R.a));
-    const T diva = A::rcp(a);
+    // std::max(a_left, a_right) takes a_right iff a_left < a_right; with K < 0 the
+    // products order the other way
+    const bool right = ph.kneg ? (R.Ka < L.Ka) : (L.Ka < R.Ka);
+    const T a = right ? R.Ka : L.Ka;
+    const T diva = right ? R.iKa : L.iKa;
     const T us = A::mul(A::half, A::sub(A::add(L.un, R.un), A::mul(diva, A::sub(R.p, L.p))));
     const T ps = A::mul(A::half, A::sub(A::add(L.p, R.p), A::mul(a, A::sub(R.un, L.un))));
     const bool up = us >= T(0);
@@ -170,16 +182,53 @@ __device__ __forceinline__ Upd2<T> update2(T ur, T uu, T uv, T uE, const Flux2<T
     o.u = A::add(A::add(uu, x_u), y_u);
     o.v = A::add(A::add(uv, x_v), y_v);
     o.E = A::add(A::add(uE, x_E), y_E);
-    const T inv = A::rcp(o.r);
-    const T qu = A::mul(o.u, inv);
-    const T qv = A::mul(o.v, inv);
+    o.speed = T(0);
+    return o;
+}
+
+// Signal speed c_s + |u| of a 2D state, hydro2d/kernel.cxx:287-309.
+template <class T> __device__ __forceinline__ T speed2(T r, T ru, T rv, T E, const Phys<T> &ph)
+{
+    using A = Ar<T>;
+    const T inv = A::rcp(r);
+    const T qu = A::mul(ru, inv);
+    const T qv = A::mul(rv, inv);
     const T temp = A::add(A::mul(qu, qu), A::mul(qv, qv));
-    const T e_int = A::sub(A::mul(o.E, inv), A::mul(A::half, temp));
-    const T p = A::mul(A::mul(ph.gm1, o.r), e_int);
+    const T e_int = A::sub(A::mul(E, inv), A::mul(A::half, temp));
+    const T p = A::mul(A::mul(ph.gm1, r), e_int);
     const T c_s = A::sqrt(A::mul(A::mul(ph.gamma, p), inv));
     const T Unorm = A::sqrt(temp);
-    o.speed = A::add(c_s, Unorm);
-    return o;
+    return A::add(c_s, Unorm);
+}
+
+// A cheap upper bound of the signal speed, for skipping cells that cannot hold the
+// maximum. Since p = (gamma-1)(E - rho|u|^2/2) <= (gamma-1) E for E, rho > 0,
+//   c_s = sqrt(gamma p / rho) <= sqrt(gamma (gamma-1) E / rho),   |u| = |rho u| / rho.
+// Evaluated in FP32 with approximate reciprocal and square root (each within a few
+// units of 2^-23), then inflated by 2^-9, far above the accumulated rounding error.
+// Returns +inf when the inputs are outside the range where the FP32 evaluation is
+// safe, and NaN when E or rho is not positive (both send the cell to the exact path).
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sqrt_approx(float x)
+{
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float speed_bound(float r, float E, float m2, float ggm1)
+{
+    // m2 = |rho u|^2 ; ggm1 = gamma * (gamma - 1)
+    if (!(r > 1e-18f) || !(r < 1e18f) || !(E > 1e-18f) || !(E < 1e18f) || !(m2 < 1e30f)) return __int_as_float(0x7f800000);
+    const float inv = rcp_approx(r);
+    const float c2 = ggm1 * E * inv;
+    const float u2 = m2 * inv * inv;
+    return (sqrt_approx(c2) + sqrt_approx(u2)) * 1.001953125f;
 }
 
 // ---------------------------------------------------------------- 3D ----------------
@@ -189,7 +238,7 @@ __device__ __forceinline__ Upd2<T> update2(T ur, T uu, T uv, T uE, const Flux2<T
 // reference's calls (hydro3d/kernel.cxx:121): x (u,v,w) and y (v,u,w) give the same sum
 // (the first addition commutes); z (w,v,u) is a different association, kept separately.
 template <class T> struct Cell3 {
-    T r, u, v, w, p, a, mu, mv, mw, eup_xy, eup_z;
+    T r, u, v, w, p, Ka, iKa, mu, mv, mw, eup_xy, eup_z;
 };
 
 template <class T>
@@ -206,7 +255,8 @@ __device__ __forceinline__ Cell3<T> make_cell3(T ur, T uu, T uv, T uw, T uE, con
     const T temp = A::add(A::add(uu2, vv2), ww2);
     const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
     c.p = A::mul(A::mul(ph.gm1, ur), e_int);
-    c.a = A::sqrt(A::mul(A::mul(ph.gamma, c.p), c.r));
+    c.Ka = A::mul(ph.K, A::sqrt(A::mul(A::mul(ph.gamma, c.p), c.r)));
+    c.iKa = A::rcp(c.Ka);
     c.mu = A::mul(c.u, c.r);
     c.mv = A::mul(c.v, c.r);
     c.mw = A::mul(c.w, c.r);
@@ -220,21 +270,21 @@ __device__ __forceinline__ Cell3<T> make_cell3(T ur, T uu, T uv, T uw, T uE, con
 // x faces: (u, v, w)
 template <class T> __device__ __forceinline__ FaceIn3<T> face3_x(const Cell3<T> &c)
 {
-    return FaceIn3<T>{c.r, c.u, c.p, c.a, c.mu, c.mv, c.mw, c.eup_xy};
+    return FaceIn3<T>{c.r, c.u, c.p, c.Ka, c.iKa, c.mu, c.mv, c.mw, c.eup_xy};
 }
 // y faces: (v, u, w)   hydro3d/kernel.cxx:254-256
 template <class T> __device__ __forceinline__ FaceIn3<T> face3_y(const Cell3<T> &c)
 {
-    return FaceIn3<T>{c.r, c.v, c.p, c.a, c.mv, c.mu, c.mw, c.eup_xy};
+    return FaceIn3<T>{c.r, c.v, c.p, c.Ka, c.iKa, c.mv, c.mu, c.mw, c.eup_xy};
 }
 // z faces: (w, v, u)   hydro3d/kernel.cxx:296-298
 template <class T> __device__ __forceinline__ FaceIn3<T> face3_z(const Cell3<T> &c)
 {
-    return FaceIn3<T>{c.r, c.w, c.p, c.a, c.mw, c.mv, c.mu, c.eup_z};
+    return FaceIn3<T>{c.r, c.w, c.p, c.Ka, c.iKa, c.mw, c.mv, c.mu, c.eup_z};
 }
 template <class T> __device__ __forceinline__ FaceIn3<T> mirror3(const FaceIn3<T> &f)
 {
-    return FaceIn3<T>{f.r, -f.un, f.p, f.a, -f.mn, f.mt1, f.mt2, f.eup};
+    return FaceIn3<T>{f.r, -f.un, f.p, f.Ka, f.iKa, -f.mn, f.mt1, f.mt2, f.eup};
 }
 
 // compute_fluxes, hydro3d/kernel.cxx:79-130
@@ -242,8 +292,9 @@ template <class T>
 __device__ __forceinline__ Flux3<T> face_flux3(const FaceIn3<T> &L, const FaceIn3<T> &R, const Phys<T> &ph)
 {
     using A = Ar<T>;
-    const T a = A::mul(ph.K, smax(L.a, R.a));
-    const T diva = A::rcp(a);
+    const bool right = ph.kneg ? (R.Ka < L.Ka) : (L.Ka < R.Ka);
+    const T a = right ? R.Ka : L.Ka;
+    const T diva = right ? R.iKa : L.iKa;
     const T us = A::mul(A::half, A::sub(A::add(L.un, R.un), A::mul(diva, A::sub(R.p, L.p))));
     const T ps = A::mul(A::half, A::sub(A::add(L.p, R.p), A::mul(a, A::sub(R.un, L.un))));
     const bool up = us >= T(0);
@@ -295,15 +346,22 @@ __device__ __forceinline__ Upd3<T> update3(T ur, T uu, T uv, T uw, T uE, const F
     o.v = A::add(A::add(A::add(uv, x_v), y_v), z_v);
     o.w = A::add(A::add(A::add(uw, x_w), y_w), z_w);
     o.E = A::add(A::add(A::add(uE, x_E), y_E), z_E);
-    const T inv = A::rcp(o.r);
-    const T qu = A::mul(o.u, inv), qv = A::mul(o.v, inv), qw = A::mul(o.w, inv);
+    o.speed = T(0);
+    return o;
+}
+
+// Signal speed c_s + |u| of a 3D state, hydro3d/kernel.cxx:367-390.
+template <class T> __device__ __forceinline__ T speed3(T r, T ru, T rv, T rw, T E, const Phys<T> &ph)
+{
+    using A = Ar<T>;
+    const T inv = A::rcp(r);
+    const T qu = A::mul(ru, inv), qv = A::mul(rv, inv), qw = A::mul(rw, inv);
     const T temp = A::add(A::add(A::mul(qu, qu), A::mul(qv, qv)), A::mul(qw, qw));
-    const T e_int = A::sub(A::mul(o.E, inv), A::mul(A::half, temp));
-    const T p = A::mul(A::mul(ph.gm1, o.r), e_int);
+    const T e_int = A::sub(A::mul(E, inv), A::mul(A::half, temp));
+    const T p = A::mul(A::mul(ph.gm1, r), e_int);
     const T c_s = A::sqrt(A::mul(A::mul(ph.gamma, p), inv));
     const T Unorm = A::sqrt(temp);
-    o.speed = A::add(c_s, Unorm);
-    return o;
+    return A::add(c_s, Unorm);
 }
 
 } // namespace hydro

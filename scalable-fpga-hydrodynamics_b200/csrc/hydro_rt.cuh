@@ -22,23 +22,45 @@ enum : unsigned {
     kErrWaitTimeout = 2u,  // a bounded wait on a TMA barrier gave up
 };
 
-// Scratch words in device memory, one set per device context. max_bits and ticket
-// are zero between launches (the last block of each launch resets them).
+// Scratch words in device memory, one set per device context. max_bits, ticket and
+// err are zero between launches (the last block of each launch resets them).
+//
+// Signal-speed skipping: a step reads the max signal speed of the previous completed
+// step of the same problem (hist_max, matched by hist_key) and computes the exact speed
+// only of cells whose cheap upper bound reaches skip_frac * hist_max. If the exact max
+// found that way is below the threshold, a skipped cell might hold the true max: the
+// step then sets `redo` and leaves Dt_next to the redo pass, which computes the exact
+// speed of every cell. Dt_next is therefore always the exact reference value.
 struct StepScratch {
     unsigned long long max_bits; // max signal speed as the bits of a non-negative double
     unsigned int ticket;         // blocks finished so far in this launch
     unsigned int err;            // error bits raised in this launch
-    double pad[2];
+    unsigned int redo;           // the last step left Dt_next to the redo pass
+    unsigned int pad0;
+    unsigned long long hist_key; // problem key of the last completed step
+    double hist_max;             // its max signal speed
 };
+
+constexpr double kSkipFrac = 0.9;
 
 // Result record of one launch, written by the last block (host-mapped memory).
 struct StepStatus {
-    double mass;      // sum of the new interior density (compensated FP64)
-    double mass_comp; // its compensation term
-    double max_speed; // max over interior cells of c_s + |u| of the new state
-    unsigned int err; // error bits
-    unsigned int seq; // launch sequence number, for the host to check completion
+    double mass;       // sum of the new interior density (compensated FP64)
+    double mass_comp;  // its compensation term
+    double max_speed;  // max over interior cells of c_s + |u| of the new state
+    unsigned int err;  // error bits
+    unsigned int seq;  // launch sequence number, for the host to check completion
+    unsigned int redo; // Dt_next still to be written by the redo pass
+    unsigned int pad;
 };
+
+// Skip threshold of a step: the previous max of the same problem, scaled.
+__device__ __forceinline__ double skip_threshold(const StepScratch *scr, unsigned long long key)
+{
+    const unsigned long long k = *reinterpret_cast<const volatile unsigned long long *>(&scr->hist_key);
+    const double m = *reinterpret_cast<const volatile double *>(&scr->hist_max);
+    return (key != 0ull && k == key) ? kSkipFrac * m : 0.0;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -132,19 +154,71 @@ struct StepAcc {
 
     template <class T> __device__ __forceinline__ void add_cell(T rho_new, T speed)
     {
+        add_mass(rho_new);
+        add_speed(speed);
+    }
+    template <class T> __device__ __forceinline__ void add_mass(T rho_new)
+    {
+        if (!(rho_new > T(0))) err |= kErrNonPhysical;
+        // Kahan step, branch-free; mc carries the low part to add back (mass = ms + mc)
+        const double y = __dadd_rn(static_cast<double>(rho_new), mc);
+        const double tt = __dadd_rn(ms, y);
+        mc = __dsub_rn(y, __dsub_rn(tt, ms));
+        ms = tt;
+    }
+    template <class T> __device__ __forceinline__ void add_speed(T speed)
+    {
         const double sp = static_cast<double>(speed);
         vmax = (sp > vmax) ? sp : vmax;
-        if (!(rho_new > T(0)) || !(sp <= 1.0e300)) err |= kErrNonPhysical;
-        neumaier_add(ms, mc, static_cast<double>(rho_new));
+        if (!(sp <= 1.0e300)) err |= kErrNonPhysical;
     }
 };
+
+// Warp + block max of non-negative doubles held as bits; result valid in thread 0.
+template <int NT> __device__ __forceinline__ unsigned long long block_max_bits(unsigned long long mb, unsigned long long *s_max)
+{
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = t & 31, warp = t >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long om = __shfl_xor_sync(0xffffffffu, mb, o);
+        mb = om > mb ? om : mb;
+    }
+    if (lane == 0) s_max[warp] = mb;
+    __syncthreads();
+    if (t == 0)
+        for (int w = 1; w < NT / 32; ++w) mb = s_max[w] > mb ? s_max[w] : mb;
+    return mb;
+}
+
+// The last block's common tail: Dt_next = C_min / max (in T, as the reference does at
+// hydro2d/kernel.cxx:318) unless the max fell below the skip threshold, the history
+// for the next step, and the re-arming of the scratch words. Thread 0 only.
+template <class T>
+__device__ __forceinline__ void finish_dt(StepScratch *scr, double vmax, double tlo, unsigned long long key, T C_min,
+                                          T *Dt_next, StepStatus *status)
+{
+    const unsigned redo = (vmax < tlo) ? 1u : 0u;
+    if (!redo) {
+        // the max of values of type T, held exactly in a double, converts back exactly
+        *Dt_next = Ar<T>::div(C_min, static_cast<T>(vmax));
+        scr->hist_key = key;
+        scr->hist_max = vmax;
+    }
+    scr->redo = redo;
+    if (status) {
+        status->max_speed = vmax;
+        status->redo = redo;
+    }
+}
 
 // Block-wide combination of the accumulators, one partial per block, one ticket atomic
 // per block; the last block writes *Dt_next = C_min / max_speed (in T, as the
 // reference does at hydro2d/kernel.cxx:318) and the status record. NT = threads/block.
 template <int NT, class T>
 __device__ __forceinline__ void step_epilogue(StepAcc acc, StepScratch *scr, double2 *partials, unsigned nblocks,
-                                              unsigned bid, T C_min, T *Dt_next, StepStatus *status, unsigned seq)
+                                              unsigned bid, T C_min, T *Dt_next, StepStatus *status, unsigned seq,
+                                              double tlo = 0.0, unsigned long long key = 0ull)
 {
     static_assert(NT % 32 == 0 && NT <= 1024, "block size");
     constexpr int NW = NT / 32;
@@ -225,12 +299,10 @@ __device__ __forceinline__ void step_epilogue(StepAcc acc, StepScratch *scr, dou
         const unsigned long long gm = atomicAdd(&scr->max_bits, 0ull);
         const unsigned gerr = atomicAdd(&scr->err, 0u);
         const double vmax = __longlong_as_double(static_cast<long long>(gm));
-        // the max of values of type T, held exactly in a double, converts back exactly
-        *Dt_next = Ar<T>::div(C_min, static_cast<T>(vmax));
+        finish_dt(scr, vmax, tlo, key, C_min, Dt_next, status);
         if (status) {
             status->mass = s;
             status->mass_comp = c;
-            status->max_speed = vmax;
             status->err = gerr;
             __threadfence_system();
             status->seq = seq;
@@ -240,6 +312,38 @@ __device__ __forceinline__ void step_epilogue(StepAcc acc, StepScratch *scr, dou
         __threadfence();
         scr->ticket = 0u;
     }
+}
+
+// Epilogue of the redo pass: the exact max over every cell, then Dt_next.
+template <int NT, class T>
+__device__ __forceinline__ void redo_epilogue(double vmax, unsigned err, StepScratch *scr, unsigned nblocks, T C_min,
+                                              T *Dt_next, StepStatus *status, unsigned long long key)
+{
+    __shared__ unsigned long long s_max[NT / 32];
+    __shared__ bool s_last;
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    err = __reduce_or_sync(0xffffffffu, err);
+    unsigned long long mb = block_max_bits<NT>(__double_as_longlong(vmax), s_max);
+    if (t == 0) {
+        atomicMax(&scr->max_bits, mb);
+        if (err) atomicOr(&scr->err, err);
+        __threadfence();
+        s_last = (atomicAdd(&scr->ticket, 1u) == nblocks - 1);
+    }
+    __syncthreads();
+    if (!s_last || t != 0) return;
+    __threadfence();
+    const unsigned long long gm = atomicAdd(&scr->max_bits, 0ull);
+    const unsigned gerr = atomicAdd(&scr->err, 0u);
+    finish_dt(scr, __longlong_as_double(static_cast<long long>(gm)), 0.0, key, C_min, Dt_next, status);
+    if (status) {
+        status->err |= gerr;
+        __threadfence_system();
+    }
+    scr->max_bits = 0ull;
+    scr->err = 0u;
+    __threadfence();
+    scr->ticket = 0u;
 }
 
 } // namespace hydro

@@ -94,6 +94,33 @@ def test_golden_runs(cuda, orc, ref_runs, kernel):
         assert orc.interior_digest(run.host_state(), run.nb) == m["sha256"], name
 
 
+@pytest.mark.parametrize("nb", [(300, 253), (20, 33, 62)])
+def test_speed_skip_redo_is_exact(cuda, oracle, nb):
+    """A step whose skip threshold comes from a much faster previous state (same Dt_next
+    and grid, so the history matches) must still return the exact Dt: the kernel skips
+    every cell, finds its max below the threshold and the redo pass recomputes it."""
+    T = np.float64
+    phys = hb.Physics(T, nb)
+    dt = cuda.zeros(1, dtype=cuda.float64, device="cuda")
+    fast = seeded_state(nb, T, 5)
+    fast[0][1::2] *= 50.0  # energy x50: signal speeds x~7
+    calm = seeded_state(nb, T, 6)
+    for st in (fast, calm):
+        oracle.ghost_x(st, nb)
+    dtd = phys.dtd(cfl_dt(phys, 0) / T(8))
+    for kernel in (hb.KERNEL_STRIP, hb.KERNEL_AUTO):
+        for sync in (True, False):
+            for st in (fast, calm):
+                cur = to_dev(cuda, st)
+                nxt = tuple(cuda.zeros_like(a) for a in cur)
+                hb.step(cur, nxt, dt, phys, dtd, kernel=kernel, sync=sync)
+                cuda.cuda.synchronize()
+                ref = (np.zeros_like(st[0]), np.zeros_like(st[1]))
+                dref = oracle.step(st, ref, phys, dtd)
+                assert T(dt.item()).tobytes() == dref.tobytes()
+                assert nxt[0].cpu().numpy().tobytes() == ref[0].tobytes()
+
+
 def test_strip_equals_direct_large(cuda):
     """Strip and direct kernels on a grid with many strips and chunks."""
     nb = (1500, 1000)
