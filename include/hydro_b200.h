@@ -112,6 +112,26 @@ int hydro3d_step_f32(const float *d_rhoE, const float *d_uvw, float *d_rhoE_next
                      size_t NB_X, size_t NB_Y, size_t NB_Z, float DtDx, float DtDy, float DtDz, void *stream,
                      int kernel, int sync, hydro_step_info_t *info);
 
+/* The 2D FP64 step of hydro2d_step_f64 for callers that cannot allocate memory.
+ * No counterpart in the reference (whose kernel needs no scratch). Some callers own all
+ * of a GPU's memory through their own pool or caching allocator, so a second allocator's
+ * cudaMalloc may fail or fragment it; others step inside a latency-critical loop where
+ * cudaMalloc/cudaFree, which can synchronise the whole device, must not run; others are
+ * built to allocate nothing after start-up. The regular entry points allocate their
+ * scratch (a few words, one partial sum per block, a pinned status record) on first use;
+ * this one allocates nothing: its scratch is a fixed array of about 1 MiB compiled into
+ * the library, which every GPU that loads the library holds until the process exits.
+ * Limit: at most 65536 blocks of partial sums per launch, i.e. NB_Y <= 8257536 (larger
+ * grids are rejected with HYDRO_ERR_ARG and a message); NB_X is handled by longer chunks.
+ * The first call on a device performs a one-time set-up (it looks up the array's device
+ * address); make that first call before any stream capture begins. All calls share the
+ * array: calls that overlap on the GPU (two streams, two threads) race and must be
+ * serialised by the caller. Arguments, results and return codes as hydro2d_step_f64. */
+int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv, double *d_rhoE_next, double *d_uv_next,
+                             double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma,
+                             double K, size_t NB_X, size_t NB_Y, double DtDx, double DtDy, void *stream, int sync,
+                             hydro_step_info_t *info);
+
 /* Results of the last step launched on the current device, for steps enqueued with
  * sync = 0: valid once the caller has synchronised that step's stream. Returns
  * HYDRO_OK, HYDRO_ERR_NONPHYSICAL or HYDRO_ERR_TIMEOUT from the step's error bits.

@@ -17,15 +17,19 @@
 //            halo column each side), marching down `chunk` rows. Each row arrives in
 //            shared memory through two TMA tile loads (one per array) into a 4-deep
 //            mbarrier ring; each lane converts its cell to primitives once, computes
-//            the x face above it and the y face to its right once (neighbours via warp
-//            shuffles, warp edges via shared memory), updates the row above, stores it
-//            with 128-bit stores and folds speed and mass into the fused epilogue.
+//            the x face above it and the y face to its right once (neighbour inputs and
+//            fluxes exchanged through shared memory with 128-bit accesses), updates the
+//            row above, stores it with 128-bit stores and folds mass, signal speed and
+//            the error checks into the fused epilogue.
 //  direct2d  one thread per cell, scalar loads of the 5-point stencil, every face
 //            evaluated from both sides like the reference. Any alignment, any size;
 //            used when the strip kernel's TMA rules do not hold and as a cross-check.
 #include <algorithm>
+#include <mutex>
+#include <stddef.h>
 #include <stdio.h>
 
+#include "../../include/hydro_b200.h"
 #include "hydro_host.h"
 
 namespace hydro {
@@ -559,3 +563,160 @@ template int mass_sum<double>(const double *, size_t, size_t, size_t, double *, 
 template int mass_sum<float>(const float *, size_t, size_t, size_t, double *, cudaStream_t);
 
 } // namespace hydro
+
+// ------------------------------------------------------------ allocation-free step ---
+// hydro2d_step_f64_noalloc: the 2D FP64 step for callers that cannot allocate device or
+// pinned host memory. All scratch of the step (the reduction words, one partial sum per
+// block, the status record) lives in the fixed array below, which every GPU that loads
+// this library holds until the process exits.
+namespace hydro {
+namespace {
+
+constexpr unsigned kNoAllocMaxBlocks = 65536; // at most this many blocks per launch
+constexpr size_t kNoAllocHeader = 256;         // StepScratch, then StepStatus
+constexpr size_t kNoAllocBytes = kNoAllocHeader + size_t(kNoAllocMaxBlocks) * sizeof(double2);
+static_assert(sizeof(StepScratch) + sizeof(StepStatus) <= kNoAllocHeader, "header layout");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_dev[64] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device.
+unsigned char *noalloc_scratch(int *rc)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+        set_error(kErrCuda, "hydro2d_step_f64_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+        *rc = kErrCuda;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_dev[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error(kErrCuda, "hydro2d_step_f64_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            *rc = kErrCuda;
+            return nullptr;
+        }
+        g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
+    }
+    *rc = kOk;
+    return g_noalloc_dev[dev];
+}
+
+} // namespace
+} // namespace hydro
+
+extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv, double *d_rhoE_next,
+                                        double *d_uv_next, double *Dt_next, double C_min, double gamma,
+                                        double gamma_minus_one, double divgamma, double K, size_t NB_X, size_t NB_Y,
+                                        double DtDx, double DtDy, void *stream, int sync, hydro_step_info_t *info)
+{
+    using namespace hydro;
+    using T = double;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!d_rhoE || !d_uv || !d_rhoE_next || !d_uv_next || !Dt_next) {
+        set_error(kErrArg, "hydro2d_step_f64_noalloc: null pointer argument");
+        return kErrArg;
+    }
+    const size_t nstrips = NB_Y == 0 ? 0 : (NB_Y + kStripW - 1) / kStripW;
+    const size_t gx_direct = NB_Y == 0 ? 0 : (NB_Y + kDirectNT - 1) / kDirectNT;
+    if (NB_X > (1u << 30) || NB_Y > (1u << 30) || nstrips > kNoAllocMaxBlocks || gx_direct > kNoAllocMaxBlocks) {
+        set_error(kErrArg,
+                  "hydro2d_step_f64_noalloc: grid %zu x %zu exceeds the fixed scratch (at most %u blocks of "
+                  "partial sums: NB_Y <= %zu)",
+                  NB_X, NB_Y, kNoAllocMaxBlocks, size_t(kStripW) * kNoAllocMaxBlocks);
+        return kErrArg;
+    }
+    int rc;
+    unsigned char *base = noalloc_scratch(&rc);
+    if (!base) return rc;
+    StepScratch *scr = reinterpret_cast<StepScratch *>(base);
+    StepStatus *status = reinterpret_cast<StepStatus *>(base + sizeof(StepScratch));
+    double2 *partials = reinterpret_cast<double2 *>(base + kNoAllocHeader);
+
+    const Phys<T> ph{C_min, gamma, gamma_minus_one, divgamma, K, K < 0.0};
+    if (NB_X == 0 || NB_Y == 0) {
+        const T dt = div_zero(C_min);
+        cudaError_t e = cudaMemcpyAsync(Dt_next, &dt, sizeof(T), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "hydro2d_step_f64_noalloc: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        if (info) *info = hydro_step_info_t{0.0, 0.0, 0u, 0};
+        return kOk;
+    }
+    // the reduction words must start at zero: clear them (the skip history after them is
+    // kept, a stale one only costs a redo pass)
+    cudaError_t e = cudaMemsetAsync(scr, 0, offsetof(StepScratch, hist_key), st);
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "hydro2d_step_f64_noalloc: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+
+    Args2<T> g;
+    g.rhoE = d_rhoE; g.uv = d_uv; g.rhoE_n = d_rhoE_next; g.uv_n = d_uv_next; g.Dt_next = Dt_next;
+    g.ph = ph; g.DtDx = DtDx; g.DtDy = DtDy;
+    g.nb_x = (int)NB_X; g.nb_y = (int)NB_Y; g.ys = (long long)NB_Y + 2;
+    g.scr = scr; g.partials = partials; g.status = status; g.seq = 0;
+    g.key = problem_key(Dt_next, NB_X, NB_Y, 0, sizeof(T), ph);
+    g.ggm1 = (float)gamma * (float)gamma_minus_one;
+
+    const size_t rowbytes = 2 * sizeof(T) * (NB_Y + 2);
+    bool strip_ok = aligned(d_rhoE, 16) && aligned(d_uv, 16) && aligned(d_rhoE_next, 16) && aligned(d_uv_next, 16) &&
+                    rowbytes % 16 == 0;
+    CUtensorMap tmr, tmu;
+    if (strip_ok)
+        strip_ok = encode_tmap_2d(&tmr, tmap_type<T>(), d_rhoE, 2 * (NB_Y + 2), NB_X + 2, rowbytes, 2 * kStripNT, 1) &&
+                   encode_tmap_2d(&tmu, tmap_type<T>(), d_uv, 2 * (NB_Y + 2), NB_X + 2, rowbytes, 2 * kStripNT, 1);
+    int kernel;
+    if (strip_ok) {
+        // as step2d, with the chunk grown until the blocks fit the fixed partials
+        const size_t max_chunks = kNoAllocMaxBlocks / nstrips;
+        const int target = 148 * 3 * 8;
+        size_t nchunks = (target + nstrips - 1) / nstrips;
+        size_t chunk = std::min<size_t>(256, std::max<size_t>(16, (NB_X + nchunks - 1) / nchunks));
+        chunk = std::max(chunk, (NB_X + std::min<size_t>(max_chunks, 65535) - 1) / std::min<size_t>(max_chunks, 65535));
+        nchunks = (NB_X + chunk - 1) / chunk;
+        g.chunk = (int)chunk;
+        strip2d<T><<<dim3((unsigned)nstrips, (unsigned)nchunks), kStripNT, 0, st>>>(tmr, tmu, g);
+        kernel = (int)Kernel::Strip;
+    } else {
+        const size_t gy = std::max<size_t>(1, std::min<size_t>({NB_X, 65535, kNoAllocMaxBlocks / gx_direct}));
+        g.chunk = 0;
+        direct2d<T><<<dim3((unsigned)gx_direct, (unsigned)gy), kDirectNT, 0, st>>>(g);
+        kernel = (int)Kernel::Direct;
+    }
+    // the redo pass returns at once unless the step left Dt_next to it
+    redo2d<T><<<148 * 4, kRedoNT, 0, st>>>(g);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "hydro2d_step_f64_noalloc launch: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    if (!sync) {
+        if (info) info->kernel = kernel;
+        return kOk;
+    }
+    StepStatus s;
+    e = cudaMemcpyAsync(&s, status, sizeof s, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "hydro2d_step_f64_noalloc: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    if (info) *info = hydro_step_info_t{s.mass + s.mass_comp, s.max_speed, s.err, kernel};
+    if (s.err & kErrWaitTimeout) {
+        set_error(kErrTimeout, "hydro2d_step_f64_noalloc: a TMA barrier wait timed out");
+        return kErrTimeout;
+    }
+    if (s.err & kErrNonPhysical) {
+        set_error(kErrPhys, "hydro2d_step_f64_noalloc: non-physical state (rho <= 0 or non-finite signal speed)");
+        return kErrPhys;
+    }
+    return kOk;
+}
