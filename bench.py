@@ -288,7 +288,10 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nb", type=int, nargs=2, default=[40000, 20000])
+    ap.add_argument("--nb", type=int, nargs="+", default=[40000, 20000],
+                    help="grid: NB_X NB_Y for 2D cases, NB_X NB_Y NB_Z for 3D cases")
+    ap.add_argument("--case", default="2d_f64", choices=["2d_f64", "2d_f32", "3d_f64", "3d_f32"],
+                    help="plain-path case timed as the headline (profiling runs pick one)")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -298,8 +301,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    nb = tuple(args.nb)
-    workload = f"2D blast {nb[0]}x{nb[1]} FP64, plain path (one launcher call per step)"
+    dim = int(args.case[0])
+    Tcase = np.float64 if args.case.endswith("f64") else np.float32
+    nb = tuple(args.nb) if len(args.nb) == dim else ((512, 512, 512) if dim == 3 else (40000, 20000))
+    workload = (f"{dim}D blast {'x'.join(map(str, nb))} {'FP64' if Tcase is np.float64 else 'FP32'}, "
+                f"plain path (one launcher call per step)")
 
     if args.impl == "reference":
         if rank != 0:
@@ -347,32 +353,34 @@ def main():
         torch.cuda.synchronize()
 
     hbm, peak_kind = peaks()
-    cells = nb[0] * nb[1]
+    cells = int(np.prod(nb))
+    isz = np.dtype(Tcase).itemsize
+    bpc = BYTES_PER_CELL[(dim, isz)]
+    kname = f"strip{dim}d<{'double' if isz == 8 else 'float'}>"
 
     barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    r = bench_resident(hb, torch, nb, np.float64, args.steps, args.warmup)
+    r = bench_resident(hb, torch, nb, Tcase, args.steps, args.warmup)
     clocks = sampler.stop()
     barrier()
     total_ms = max_over_ranks(r["total_ms"])
     ms_step = total_ms / args.steps
     value = world * cells * args.steps / (total_ms / 1e3) / 1e9
     kern_ms = statistics.mean(r["kernel_ms"])
-    achieved = cells * BYTES_PER_CELL[(2, 8)] / (kern_ms / 1e3) / 1e9
+    achieved = cells * bpc / (kern_ms / 1e3) / 1e9
     roofline = dict(bound="hbm", achieved=achieved, peak=hbm, unit="GB/s", frac=achieved / hbm,
-                    peak_kind=peak_kind, traffic=None, kernel="strip2d<double>",
-                    bytes_per_cell=BYTES_PER_CELL[(2, 8)], kernel_ms=kern_ms)
+                    peak_kind=peak_kind, traffic=None, kernel=kname, bytes_per_cell=bpc, kernel_ms=kern_ms)
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
-        tr = json.loads(tp.read_text()).get("strip2d_f64_bytes_per_cell")
+        tr = json.loads(tp.read_text()).get(f"{kname}_dram_bytes_per_cell")
         if tr:
             roofline["traffic"] = tr * cells
 
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and dim == 2:
         barrier()
-        e = bench_e2e(hb, torch, nb, np.float64, max(3, args.steps // 3), 2)
+        e = bench_e2e(hb, torch, nb, Tcase, max(3, args.steps // 3), 2)
         barrier()
         e_ms = max_over_ranks(e["ms"])
         nst = max(3, args.steps // 3)
@@ -380,7 +388,7 @@ def main():
                    d2h_bytes_per_step=e["d2h"], path="drop-in launcher (C ABI) + reference host-loop copies")
 
     variants = {}
-    if not args.no_variants:
+    if not args.no_variants and args.case == "2d_f64":
         for name, vnb, T in (("2d_f32_40000x20000", nb, np.float32), ("3d_f64_512^3", (512, 512, 512), np.float64),
                              ("3d_f32_512^3", (512, 512, 512), np.float32)):
             barrier()
@@ -396,7 +404,7 @@ def main():
                                   kernel=int(vr["kernel"]), ms_per_step=vms / nst)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and dim == 2:
         thr = cpu_threads()
         rate, kind, what = cpu_reference_sample(nb[1], 32, 3.0, thr)
         cpu = dict(value=rate / 1e9, unit=UNIT, cores=thr, kind=kind,
@@ -404,9 +412,10 @@ def main():
 
     if rank == 0:
         line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
-                    ms_per_step=ms_step, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
-                    data="synthetic (reference blast IC, built on the device)",
-                    config=dict(workload=workload, nb_x=nb[0], nb_y=nb[1], l2="inputs larger than L2 (51.2 GB)",
+                    ms_per_step=ms_step, higher_is_better=True, scaling="weak", vs_baseline=None,
+                    dtype="f64" if isz == 8 else "f32", data="synthetic (reference blast IC, built on the device)",
+                    config=dict(workload=workload, nb=list(nb),
+                                l2=f"inputs larger than L2 ({cells * bpc / 2 / 1e9:.1f} GB state, 126 MB L2)",
                                 parallelism=f"replicas x{world}"),
                     roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps, clocks=clocks,
                     variants=variants)

@@ -170,12 +170,17 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
     T Ur = 0, Uu = 0, Uv = 0, Uw = 0, UE = 0;
     Flux3<T> fxlo{};
     const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
+    // ghost cells (j or k = 0 or NB+1) and cells past the array are never used: they
+    // convert a unit state so every lane's reciprocal / square root stays regular
+    const bool real = (j >= 1) && (j <= g.nb_y) && (k >= 1) && (k <= g.nb_z);
+#pragma unroll 2
     for (int m = 0; m < nplanes; ++m) {
         issue(m + k3Stages - 1);
         cp_async_wait<k3Stages - 1>();
         const int s = m % k3Stages;
-        const T ur = S.st[s][0][t], uE = S.st[s][1][t], uu = S.st[s][2][t], uv = S.st[s][3][t],
-                uw = S.st[s][4][t];
+        const T ur = real ? S.st[s][0][t] : T(1), uE = real ? S.st[s][1][t] : T(1);
+        const T uu = real ? S.st[s][2][t] : T(0), uv = real ? S.st[s][3][t] : T(0);
+        const T uw = real ? S.st[s][4][t] : T(0);
         const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, g.ph);
         {
             const FaceIn3<T> fy = face3_y(P);
