@@ -160,6 +160,61 @@ int hydro3d_init_blast_f32(float *d_rhoE, float *d_uvw, size_t NB_X, size_t NB_Y
 int hydro_mass_f64(const double *d_rhoE, size_t NB_X, size_t NB_Y, size_t NB_Z, double *out, void *stream);
 int hydro_mass_f32(const float *d_rhoE, size_t NB_X, size_t NB_Y, size_t NB_Z, double *out, void *stream);
 
+/* ---- batched step ----------------------------------------------------------------------- */
+/* No counterpart in the reference, whose host loop advances one domain per rank
+ * (hydro2d/main.cxx:689-815): many independent blast instances of uneven sizes advanced by
+ * one persistent kernel per step, each with its own Dt, simulated time (FP64), end time
+ * and conservation sums; n steps run as one CUDA graph with no host round trip. An
+ * instance's state is bit-identical to the same blast advanced alone (or through the plain
+ * path) in the same precision. */
+
+/* One blast problem. Cell-index coordinates as the reference's initial condition uses them
+ * (interior cells 1..NB per axis, hydro2d/main.cxx:290-306): density rho_in / pressure
+ * p_in inside the circle (sphere) of `radius` around `centre`, rho_out / p_out outside,
+ * at rest; gamma, K and the CFL number C as hydro2d/main.cxx:601-607. The instance runs
+ * while t < t_end and steps < max_steps (the reference loop condition, main.cxx:689). */
+typedef struct hydro_blast {
+    size_t nb[3]; /* NB_X, NB_Y, NB_Z (NB_Z = 0 in 2D) */
+    double centre[3];
+    double radius;
+    double rho_in, rho_out, p_in, p_out;
+    double gamma, K, C;
+    double t_end;
+    long long max_steps;
+} hydro_blast_t;
+
+typedef struct hydro_batch_status {
+    double t, dt;      /* simulated time reached; the Dt of the next step */
+    double mass;       /* compensated FP64 sums over the interior after the last step */
+    double mom[3];
+    double energy;
+    double max_speed;
+    long long steps;
+    int active;        /* 0 once t >= t_end, steps >= max_steps or an error */
+    unsigned err;      /* bit 0: non-physical state; bit 1: a bounded wait timed out */
+} hydro_batch_status_t;
+
+/* A batch of `dim`-D (2) instances in FP32 (precision_bytes 4) or FP64 (8), rows per work
+ * item `chunk` (0: default), at most `capacity` instances, on `stream` (NULL: its own). */
+void *hydro_batch_create(int dim, int precision_bytes, int chunk, int capacity, void *stream);
+/* Allocate, initialise and admit one instance; returns its slot (>= 0) or an error code. */
+int hydro_batch_add(void *batch, const hydro_blast_t *spec);
+/* Device bytes one instance of `spec` holds (state, double-buffered). */
+long long hydro_batch_bytes(void *batch, const hydro_blast_t *spec);
+/* Release an instance's slot and memory (waits for the batch's stream). */
+int hydro_batch_remove(void *batch, int slot);
+/* Enqueue `nsteps` batched steps (one CUDA graph); sync = 1 waits for them. */
+int hydro_batch_run(void *batch, int nsteps, int sync);
+/* An instance's status after the last completed step (valid once the batch is synced). */
+int hydro_batch_status(void *batch, int slot, hydro_batch_status_t *out);
+/* Device pointers to an instance's current (rho,E) and momentum arrays and their row
+ * stride in cells (rows may be padded past NB_Y + 2). Valid until the next run. */
+int hydro_batch_state(void *batch, int slot, const void **rhoE, const void **uvx, long long *row_stride);
+/* Copy an instance's current state into caller buffers in the reference layout
+ * ((NB_X+2)(NB_Y+2) cells, no row padding); `to_host` selects host or device buffers. */
+int hydro_batch_copy_state(void *batch, int slot, void *rhoE, void *uvx, int to_host);
+void hydro_batch_destroy(void *batch);
+
 /* ---- errors -------------------------------------------------------------------------- */
 /* No counterpart in the reference (it has no status return): last error code latched
  * by any entry point (0 = none), its message, and a reset. */

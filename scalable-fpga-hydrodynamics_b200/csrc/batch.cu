@@ -1,0 +1,664 @@
+// Batched step: many independent 2D blast instances of uneven sizes advanced by one
+// persistent kernel per step, each instance with its own time step, boundaries and
+// simulated time (the layered "batching" change of the plain path; no counterpart in the
+// reference, whose host loop advances one domain, hydro2d/main.cxx:689-815).
+//
+// Each instance keeps the plain path's layout (two interleaved-pair arrays with ghosts,
+// double-buffered) and the plain path's arithmetic: the same strip march
+// (strip2d_march.cuh), so an instance's state after n batched steps is bit-identical to n
+// plain steps. Work is a flat list of (instance, strip x chunk) items; persistent blocks
+// take items from an atomic counter. Every item writes its partial sums (compensated FP64
+// mass, momenta and energy; max signal speed; error bits) to its own slot; the item that
+// completes an instance's step (ticket per instance) merges that instance's slots in
+// item order -- the result does not depend on which block ran which item, nor on the
+// other instances in the batch -- and advances the instance on the device:
+//   Dt = min(1e20, C_min / max_speed)   (hydro2d/kernel.cxx:318, main.cxx:706-781)
+//   t += Dt (FP64 accumulator), DtDx = Dt / DX, DtDy = Dt / DY (main.cxx:703-704, in T)
+//   active while t < t_end and steps < max_steps (main.cxx:689)
+// so a step needs no host round trip and n steps are captured as one CUDA graph.
+#include <algorithm>
+#include <mutex>
+#include <stdio.h>
+#include <string.h>
+#include <vector>
+
+#include "../../include/hydro_b200.h"
+#include "hydro_host.h"
+#include "strip2d_march.cuh"
+
+namespace hydro {
+
+constexpr int kSums = 5; // rho, rho u, rho v, rho w (0 in 2D), E
+
+template <class T> struct alignas(128) Inst2 {
+    CUtensorMap tm[2][2]; // [buffer][0: (rho, E), 1: (rho u, rho v)]
+    T *rhoE[2], *uv[2];
+    Phys<T> ph;
+    T DX, DY, dt, DtDx, DtDy;
+    double t, t_end;
+    long long ys;
+    long long steps, max_steps;
+    int nb_x, nb_y, nstrips, chunk;
+    int parity, active;
+    unsigned done_items, err;
+};
+
+struct ItemPart {
+    double s[kSums], c[kSums];
+    unsigned long long maxbits;
+    unsigned err, pad;
+};
+
+// per-slot status, host-mapped, written by the finalising item
+struct SlotStatus {
+    double t, dt, sums[kSums], max_speed;
+    long long steps;
+    int active;
+    unsigned err;
+};
+
+struct BatchAcc {
+    double s[kSums] = {0, 0, 0, 0, 0}, c[kSums] = {0, 0, 0, 0, 0};
+    double vmax = 0.0;
+    unsigned err = 0;
+
+    __device__ __forceinline__ void kahan(int q, double x)
+    {
+        const double y = __dadd_rn(x, c[q]);
+        const double tt = __dadd_rn(s[q], y);
+        c[q] = __dsub_rn(y, __dsub_rn(tt, s[q]));
+        s[q] = tt;
+    }
+    template <class T> __device__ __forceinline__ void add(T r, T mu, T mv, T mw, T E, T speed)
+    {
+        kahan(0, (double)r);
+        kahan(1, (double)mu);
+        kahan(2, (double)mv);
+        kahan(3, (double)mw);
+        kahan(4, (double)E);
+        const double sp = (double)speed;
+        vmax = (sp > vmax) ? sp : vmax;
+        if (!(r > T(0)) || !(sp <= 1.0e300)) err |= kErrNonPhysical;
+    }
+};
+
+// deterministic merge of (s, c) pairs: the lower lane's value first
+__device__ __forceinline__ void merge_pair(double &s, double &c, double s2, double c2, bool upper)
+{
+    if (upper) {
+        double a = s2, b = c2;
+        neumaier_merge(a, b, s, c);
+        s = a;
+        c = b;
+    } else {
+        neumaier_merge(s, c, s2, c2);
+    }
+}
+
+// Block-wide reduction of a BatchAcc; the result is valid in thread 0.
+template <int NT> __device__ __forceinline__ void block_reduce(BatchAcc &a)
+{
+    constexpr int NW = NT / 32;
+    __shared__ double r_s[NW][kSums], r_c[NW][kSums];
+    __shared__ unsigned long long r_m[NW];
+    __shared__ unsigned r_e[NW];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    unsigned long long mb = __double_as_longlong(a.vmax);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int q = 0; q < kSums; ++q) {
+            const double s2 = __shfl_xor_sync(0xffffffffu, a.s[q], o);
+            const double c2 = __shfl_xor_sync(0xffffffffu, a.c[q], o);
+            merge_pair(a.s[q], a.c[q], s2, c2, up);
+        }
+        const unsigned long long om = __shfl_xor_sync(0xffffffffu, mb, o);
+        mb = om > mb ? om : mb;
+        a.err |= __shfl_xor_sync(0xffffffffu, a.err, o);
+    }
+    if (lane == 0) {
+        for (int q = 0; q < kSums; ++q) {
+            r_s[warp][q] = a.s[q];
+            r_c[warp][q] = a.c[q];
+        }
+        r_m[warp] = mb;
+        r_e[warp] = a.err;
+    }
+    __syncthreads();
+    if (t == 0) {
+        for (int w = 1; w < NW; ++w) {
+            for (int q = 0; q < kSums; ++q) neumaier_merge(a.s[q], a.c[q], r_s[w][q], r_c[w][q]);
+            mb = r_m[w] > mb ? r_m[w] : mb;
+            a.err |= r_e[w];
+        }
+        a.vmax = __longlong_as_double((long long)mb);
+    }
+    __syncthreads();
+}
+
+// Merge an instance's item slots in item order and advance the instance (whole block).
+template <int NT, class T>
+__device__ void finalize_instance(Inst2<T> *I, const ItemPart *parts, int nitems, SlotStatus *st)
+{
+    BatchAcc a;
+    unsigned long long mb = 0ull;
+    for (int i = threadIdx.x; i < nitems; i += NT) {
+        const ItemPart &p = parts[i];
+        for (int q = 0; q < kSums; ++q) neumaier_merge(a.s[q], a.c[q], __ldcg(&p.s[q]), __ldcg(&p.c[q]));
+        const unsigned long long m = __ldcg(&p.maxbits);
+        mb = m > mb ? m : mb;
+        a.err |= __ldcg(&p.err);
+    }
+    a.vmax = __longlong_as_double((long long)mb);
+    block_reduce<NT>(a);
+    if (threadIdx.x == 0) {
+        using A = Ar<T>;
+        const T big = T(1e20);
+        const T dtn = A::div(I->ph.C_min, static_cast<T>(a.vmax));
+        const T Dt = (dtn < big) ? dtn : big;
+        I->steps += 1;
+        I->t = __dadd_rn(I->t, (double)Dt);
+        I->dt = Dt;
+        I->DtDx = A::div(Dt, I->DX);
+        I->DtDy = A::div(Dt, I->DY);
+        I->parity ^= 1;
+        I->err |= a.err;
+        I->active = (I->t < I->t_end) && (I->steps < I->max_steps) && !(I->err & kErrNonPhysical);
+        if (st) {
+            st->t = I->t;
+            st->dt = (double)Dt;
+            for (int q = 0; q < kSums; ++q) st->sums[q] = __dadd_rn(a.s[q], a.c[q]);
+            st->max_speed = a.vmax;
+            st->steps = I->steps;
+            st->active = I->active;
+            st->err = I->err;
+        }
+        __threadfence();
+        I->done_items = 0;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kStripNT, 4) batch2d(Inst2<T> *insts, const int2 *items, const int2 *ranges,
+                                                      int nitems, unsigned *counter, ItemPart *parts,
+                                                      SlotStatus *status)
+{
+    __shared__ Smem2<T> S;
+    __shared__ int s_item;
+    __shared__ int s_last;
+    march2d_init(S);
+    unsigned ld = 0;
+    for (;;) {
+        __syncthreads(); // everyone has read s_item / finished the previous item
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int w = s_item;
+        if (w >= nitems) break;
+        const int2 it = items[w];
+        Inst2<T> *I = insts + it.x;
+        if (!I->active) continue;
+        const int par = I->parity;
+        const int strip = it.y % I->nstrips, ck = it.y / I->nstrips;
+        const int i0 = 1 + ck * I->chunk;
+        const March2 geo{kStripW * strip, i0, min(i0 + I->chunk - 1, I->nb_x), I->nb_x, I->nb_y, I->ys};
+        const Phys<T> ph = I->ph;
+        if (threadIdx.x == 0) {
+            prefetch_tensormap(&I->tm[par][0]);
+            prefetch_tensormap(&I->tm[par][1]);
+        }
+        BatchAcc acc;
+        const bool ok = march2d<T>(S, &I->tm[par][0], &I->tm[par][1], geo, I->rhoE[par ^ 1], I->uv[par ^ 1], ph,
+                                   I->DtDx, I->DtDy, ld, [&](const Upd2<T> &o) {
+                                       acc.add(o.r, o.u, o.v, T(0), o.E, speed2(o.r, o.u, o.v, o.E, ph));
+                                   });
+        if (!ok) acc.err |= kErrWaitTimeout;
+        block_reduce<kStripNT>(acc);
+        if (threadIdx.x == 0) {
+            ItemPart &p = parts[w];
+            for (int q = 0; q < kSums; ++q) {
+                p.s[q] = acc.s[q];
+                p.c[q] = acc.c[q];
+            }
+            p.maxbits = (unsigned long long)__double_as_longlong(acc.vmax);
+            p.err = acc.err;
+            __threadfence();
+            const int2 rg = ranges[it.x];
+            s_last = (atomicAdd(&I->done_items, 1u) == (unsigned)rg.y - 1u);
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const int2 rg = ranges[it.x];
+            finalize_instance<kStripNT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr);
+        }
+    }
+}
+
+// ----------------------------------------------------------------------- host engine ---
+class BatchBase {
+  public:
+    virtual ~BatchBase() = default;
+    virtual int add(const hydro_blast_t &spec) = 0;
+    virtual int remove(int slot) = 0;
+    virtual int run(int nsteps, bool sync) = 0;
+    virtual int status(int slot, hydro_batch_status_t *out) = 0;
+    virtual int state(int slot, const void **rhoE, const void **uvx, long long *row_stride) = 0;
+    virtual size_t bytes(const hydro_blast_t &spec) const = 0;
+    virtual int copy_state(int slot, void *rhoE, void *uvx, bool to_host) = 0;
+};
+
+template <class T> class Batch2 final : public BatchBase {
+  public:
+    Batch2(int chunk, int capacity, cudaStream_t stream, int *rc) : chunk_(chunk > 0 ? chunk : 128), cap_(capacity)
+    {
+        own_stream_ = (stream == nullptr);
+        cudaError_t e = cudaSuccess;
+        if (own_stream_) e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+        else stream_ = stream;
+        if (e == cudaSuccess) e = cudaMalloc(&insts_, sizeof(Inst2<T>) * cap_);
+        if (e == cudaSuccess) e = cudaMalloc(&ranges_, sizeof(int2) * cap_);
+        if (e == cudaSuccess) e = cudaMalloc(&counter_, 64);
+        if (e == cudaSuccess) e = cudaMalloc(&scratch_bits_, 64);
+        if (e == cudaSuccess) e = cudaMemset(scratch_bits_, 0, 64);
+        if (e == cudaSuccess) e = cudaHostAlloc(&status_h_, sizeof(SlotStatus) * cap_, cudaHostAllocMapped);
+        if (e == cudaSuccess) e = cudaHostGetDevicePointer(&status_d_, status_h_, 0);
+        if (e == cudaSuccess) memset(status_h_, 0, sizeof(SlotStatus) * cap_);
+        int dev = 0, nsm = 148, occ = 4;
+        if (e == cudaSuccess) e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch2d<T>, kStripNT, 0);
+        blocks_ = nsm * std::max(1, occ);
+        slots_.resize(cap_);
+        host_ranges_.assign(cap_, make_int2(0, 0));
+        *rc = (e == cudaSuccess) ? kOk : kErrCuda;
+        if (e != cudaSuccess) set_error(kErrCuda, "batch create: %s", cudaGetErrorString(e));
+    }
+
+    ~Batch2() override
+    {
+        if (graph_) cudaGraphExecDestroy(graph_);
+        for (auto &s : slots_)
+            if (s.used) free_slot(s);
+        cudaFree(insts_);
+        cudaFree(ranges_);
+        cudaFree(counter_);
+        cudaFree(scratch_bits_);
+        cudaFree(items_);
+        cudaFree(parts_);
+        cudaFreeHost(status_h_);
+        if (own_stream_) cudaStreamDestroy(stream_);
+    }
+
+    static size_t row_stride(size_t nb_y)
+    {
+        const size_t per = 16 / (2 * sizeof(T)); // cells per 16 bytes of one pair array
+        return (nb_y + 2 + per - 1) / per * per;
+    }
+
+    size_t bytes(const hydro_blast_t &s) const override
+    {
+        return 2 * 4 * sizeof(T) * (s.nb[0] + 2) * row_stride(s.nb[1]);
+    }
+
+    int add(const hydro_blast_t &s) override
+    {
+        const size_t nb_x = s.nb[0], nb_y = s.nb[1];
+        if (nb_x == 0 || nb_y == 0 || nb_x > (1u << 24) || nb_y > (1u << 24) || !(s.gamma > 1.0)) {
+            set_error(kErrArg, "batch add: invalid blast (grid %zu x %zu, gamma %g)", nb_x, nb_y, s.gamma);
+            return kErrArg;
+        }
+        // the batch owns its layout: rows are padded to a 16-byte multiple (one spare
+        // cell for odd NB_Y in FP32) so that every instance can be fed by TMA
+        const size_t ys = row_stride(nb_y), rowbytes = 2 * sizeof(T) * ys;
+        int slot = -1;
+        for (int i = 0; i < cap_; ++i)
+            if (!slots_[i].used) {
+                slot = i;
+                break;
+            }
+        if (slot < 0) {
+            set_error(kErrArg, "batch add: all %d slots are in use", cap_);
+            return kErrArg;
+        }
+        Slot &sl = slots_[slot];
+        const size_t n = 2 * ys * (nb_x + 2);
+        cudaError_t e = cudaSuccess;
+        for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+            e = cudaMallocAsync(&sl.rhoE[b], n * sizeof(T), stream_);
+            if (e == cudaSuccess) e = cudaMallocAsync(&sl.uv[b], n * sizeof(T), stream_);
+            if (e == cudaSuccess) e = cudaMemsetAsync(sl.rhoE[b], 0, n * sizeof(T), stream_);
+            if (e == cudaSuccess) e = cudaMemsetAsync(sl.uv[b], 0, n * sizeof(T), stream_);
+        }
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "batch add: allocation of %zu bytes failed: %s", bytes(s), cudaGetErrorString(e));
+            for (int b = 0; b < 2; ++b) {
+                if (sl.rhoE[b]) cudaFreeAsync(sl.rhoE[b], stream_);
+                if (sl.uv[b]) cudaFreeAsync(sl.uv[b], stream_);
+                sl.rhoE[b] = sl.uv[b] = nullptr;
+            }
+            return kErrCuda;
+        }
+        Inst2<T> I;
+        memset(&I, 0, sizeof I);
+        const T one = T(1);
+        I.DX = one / T(nb_x + 1);
+        I.DY = one / T(nb_y + 1);
+        const T ms = (I.DY < I.DX) ? I.DY : I.DX;
+        I.ph.C_min = T(T(s.C) * ms);
+        I.ph.gamma = T(s.gamma);
+        I.ph.gm1 = T(I.ph.gamma - one);
+        I.ph.divgamma = T(one / I.ph.gm1);
+        I.ph.K = T(s.K);
+        I.ph.kneg = I.ph.K < T(0);
+        T first = 0;
+        int rc = init2d_at<T>(sl.rhoE[0], sl.uv[0], nb_x, nb_y, s.centre[0], s.centre[1], s.radius, T(s.rho_in),
+                              T(s.rho_out), T(s.p_in), T(s.p_out), I.ph.C_min, I.ph.gamma, &first, stream_,
+                              scratch_bits_, (long long)ys);
+        if (rc != kOk) {
+            free_slot(sl);
+            return rc;
+        }
+        const T big = T(1e20);
+        I.dt = (first < big) ? first : big; // first_Dt = min(1e20, IC min), main.cxx:618-660
+        I.DtDx = I.dt / I.DX;
+        I.DtDy = I.dt / I.DY;
+        I.t = 0.0;
+        I.t_end = s.t_end;
+        I.max_steps = s.max_steps;
+        I.steps = 0;
+        I.nb_x = (int)nb_x;
+        I.nb_y = (int)nb_y;
+        I.ys = (long long)ys;
+        I.nstrips = (int)((nb_y + kStripW - 1) / kStripW);
+        I.chunk = chunk_;
+        I.parity = 0;
+        I.active = (0.0 < s.t_end) && (0 < s.max_steps);
+        for (int b = 0; b < 2; ++b) {
+            I.rhoE[b] = sl.rhoE[b];
+            I.uv[b] = sl.uv[b];
+            const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+            if (!encode_tmap_2d(&I.tm[b][0], dt, sl.rhoE[b], 2 * ys, nb_x + 2, rowbytes, 2 * kStripNT, 1) ||
+                !encode_tmap_2d(&I.tm[b][1], dt, sl.uv[b], 2 * ys, nb_x + 2, rowbytes, 2 * kStripNT, 1)) {
+                free_slot(sl);
+                set_error(kErrCuda, "batch add: tensor map encoding failed");
+                return kErrCuda;
+            }
+        }
+        e = cudaMemcpyAsync(insts_ + slot, &I, sizeof I, cudaMemcpyHostToDevice, stream_);
+        SlotStatus st0{};
+        st0.dt = (double)I.dt;
+        st0.active = I.active;
+        status_h_[slot] = st0;
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) {
+            free_slot(sl);
+            set_error(kErrCuda, "batch add: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        sl.used = true;
+        sl.nitems = I.nstrips * (int)((nb_x + chunk_ - 1) / chunk_);
+        sl.bytes = bytes(s);
+        sl.ys = ys;
+        sl.nb_x = nb_x;
+        sl.nb_y = nb_y;
+        dirty_ = true;
+        return slot;
+    }
+
+    int remove(int slot) override
+    {
+        if (slot < 0 || slot >= cap_ || !slots_[slot].used) {
+            set_error(kErrArg, "batch remove: no instance in slot %d", slot);
+            return kErrArg;
+        }
+        cudaError_t e = cudaStreamSynchronize(stream_);
+        free_slot(slots_[slot]);
+        dirty_ = true;
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "batch remove: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        return kOk;
+    }
+
+    int run(int nsteps, bool sync) override
+    {
+        if (nsteps < 0) {
+            set_error(kErrArg, "batch run: negative step count");
+            return kErrArg;
+        }
+        int rc = kOk;
+        if (dirty_ || nsteps != graph_steps_) rc = rebuild(nsteps);
+        if (rc != kOk) return rc;
+        cudaError_t e = cudaSuccess;
+        if (nitems_ > 0 && nsteps > 0) e = cudaGraphLaunch(graph_, stream_);
+        if (e == cudaSuccess && sync) e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "batch run: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        return kOk;
+    }
+
+    int status(int slot, hydro_batch_status_t *out) override
+    {
+        if (slot < 0 || slot >= cap_ || !slots_[slot].used || !out) {
+            set_error(kErrArg, "batch status: no instance in slot %d", slot);
+            return kErrArg;
+        }
+        const volatile SlotStatus *v = status_h_ + slot;
+        out->t = v->t;
+        out->dt = v->dt;
+        out->mass = v->sums[0];
+        out->mom[0] = v->sums[1];
+        out->mom[1] = v->sums[2];
+        out->mom[2] = v->sums[3];
+        out->energy = v->sums[4];
+        out->max_speed = v->max_speed;
+        out->steps = v->steps;
+        out->active = v->active;
+        out->err = v->err;
+        return kOk;
+    }
+
+    int state(int slot, const void **rhoE, const void **uvx, long long *row_stride) override
+    {
+        if (slot < 0 || slot >= cap_ || !slots_[slot].used) {
+            set_error(kErrArg, "batch state: no instance in slot %d", slot);
+            return kErrArg;
+        }
+        // the current buffer is the one the last completed step wrote: parity of steps
+        const int par = (int)(status_h_[slot].steps & 1);
+        *rhoE = slots_[slot].rhoE[par];
+        *uvx = slots_[slot].uv[par];
+        if (row_stride) *row_stride = (long long)slots_[slot].ys;
+        return kOk;
+    }
+
+    int copy_state(int slot, void *rhoE, void *uvx, bool to_host) override
+    {
+        const void *r, *u;
+        long long ys;
+        int rc = state(slot, &r, &u, &ys);
+        if (rc != kOk) return rc;
+        const Slot &sl = slots_[slot];
+        const size_t w = 2 * sizeof(T) * (sl.nb_y + 2), sp = 2 * sizeof(T) * (size_t)ys;
+        const cudaMemcpyKind k = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+        cudaError_t e = cudaMemcpy2DAsync(rhoE, w, r, sp, w, sl.nb_x + 2, k, stream_);
+        if (e == cudaSuccess) e = cudaMemcpy2DAsync(uvx, w, u, sp, w, sl.nb_x + 2, k, stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "batch copy_state: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        return kOk;
+    }
+
+  private:
+    struct Slot {
+        bool used = false;
+        T *rhoE[2] = {nullptr, nullptr}, *uv[2] = {nullptr, nullptr};
+        int nitems = 0;
+        size_t bytes = 0;
+        size_t ys = 0, nb_x = 0, nb_y = 0;
+    };
+
+    void free_slot(Slot &s)
+    {
+        for (int b = 0; b < 2; ++b) {
+            if (s.rhoE[b]) cudaFreeAsync(s.rhoE[b], stream_);
+            if (s.uv[b]) cudaFreeAsync(s.uv[b], stream_);
+            s.rhoE[b] = s.uv[b] = nullptr;
+        }
+        s.used = false;
+        s.nitems = 0;
+    }
+
+    // Work list and partial slots for the instances in use; the graph of `nsteps` steps.
+    int rebuild(int nsteps)
+    {
+        std::vector<int2> items;
+        for (int i = 0; i < cap_; ++i) {
+            if (!slots_[i].used) {
+                host_ranges_[i] = make_int2(0, 0);
+                continue;
+            }
+            host_ranges_[i] = make_int2((int)items.size(), slots_[i].nitems);
+            for (int k = 0; k < slots_[i].nitems; ++k) items.push_back(make_int2(i, k));
+        }
+        cudaError_t e = cudaStreamSynchronize(stream_);
+        if (e == cudaSuccess && items.size() > items_cap_) {
+            cudaFree(items_);
+            cudaFree(parts_);
+            items_ = nullptr;
+            parts_ = nullptr;
+            items_cap_ = std::max(items.size(), 2 * items_cap_);
+            e = cudaMalloc(&items_, sizeof(int2) * items_cap_);
+            if (e == cudaSuccess) e = cudaMalloc(&parts_, sizeof(ItemPart) * items_cap_);
+            if (e != cudaSuccess) items_cap_ = 0;
+        }
+        nitems_ = (int)items.size();
+        if (e == cudaSuccess && nitems_ > 0)
+            e = cudaMemcpyAsync(items_, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, stream_);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ranges_, host_ranges_.data(), sizeof(int2) * cap_, cudaMemcpyHostToDevice, stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+        if (graph_) {
+            cudaGraphExecDestroy(graph_);
+            graph_ = nullptr;
+        }
+        if (e == cudaSuccess && nitems_ > 0 && nsteps > 0) {
+            cudaGraph_t g = nullptr;
+            e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal);
+            for (int k = 0; k < nsteps && e == cudaSuccess; ++k) {
+                e = cudaMemsetAsync(counter_, 0, sizeof(unsigned), stream_);
+                if (e == cudaSuccess) {
+                    batch2d<T><<<blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
+                                                                 status_d_);
+                    e = cudaGetLastError();
+                }
+            }
+            const cudaError_t e2 = cudaStreamEndCapture(stream_, &g);
+            if (e == cudaSuccess) e = e2;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_, g, 0);
+            if (g) cudaGraphDestroy(g);
+        }
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "batch rebuild: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        dirty_ = false;
+        graph_steps_ = nsteps;
+        return kOk;
+    }
+
+    int chunk_, cap_;
+    bool own_stream_ = false, dirty_ = true;
+    cudaStream_t stream_ = nullptr;
+    Inst2<T> *insts_ = nullptr;
+    int2 *ranges_ = nullptr, *items_ = nullptr;
+    size_t items_cap_ = 0;
+    ItemPart *parts_ = nullptr;
+    unsigned *counter_ = nullptr;
+    unsigned long long *scratch_bits_ = nullptr;
+    SlotStatus *status_h_ = nullptr, *status_d_ = nullptr;
+    std::vector<Slot> slots_;
+    std::vector<int2> host_ranges_;
+    int nitems_ = 0, blocks_ = 148, graph_steps_ = -1;
+    cudaGraphExec_t graph_ = nullptr;
+};
+
+} // namespace hydro
+
+using namespace hydro;
+
+extern "C" {
+
+void *hydro_batch_create(int dim, int precision_bytes, int chunk, int capacity, void *stream)
+{
+    if (dim != 2 || (precision_bytes != 4 && precision_bytes != 8) || capacity <= 0 || capacity > (1 << 20) ||
+        chunk < 0) {
+        set_error(kErrArg, "hydro_batch_create: unsupported (dim %d, precision %d bytes, capacity %d)", dim,
+                  precision_bytes, capacity);
+        return nullptr;
+    }
+    int rc = kOk;
+    BatchBase *b = nullptr;
+    if (precision_bytes == 8) b = new Batch2<double>(chunk, capacity, (cudaStream_t)stream, &rc);
+    else b = new Batch2<float>(chunk, capacity, (cudaStream_t)stream, &rc);
+    if (rc != kOk) {
+        delete b;
+        return nullptr;
+    }
+    return b;
+}
+
+int hydro_batch_add(void *b, const hydro_blast_t *spec)
+{
+    if (!b || !spec) {
+        set_error(kErrArg, "hydro_batch_add: null argument");
+        return kErrArg;
+    }
+    return static_cast<BatchBase *>(b)->add(*spec);
+}
+
+int hydro_batch_remove(void *b, int slot)
+{
+    if (!b) return kErrArg;
+    return static_cast<BatchBase *>(b)->remove(slot);
+}
+
+int hydro_batch_run(void *b, int nsteps, int sync)
+{
+    if (!b) return kErrArg;
+    return static_cast<BatchBase *>(b)->run(nsteps, sync != 0);
+}
+
+int hydro_batch_status(void *b, int slot, hydro_batch_status_t *out)
+{
+    if (!b) return kErrArg;
+    return static_cast<BatchBase *>(b)->status(slot, out);
+}
+
+int hydro_batch_state(void *b, int slot, const void **rhoE, const void **uvx, long long *row_stride)
+{
+    if (!b || !rhoE || !uvx) return kErrArg;
+    return static_cast<BatchBase *>(b)->state(slot, rhoE, uvx, row_stride);
+}
+
+long long hydro_batch_bytes(void *b, const hydro_blast_t *spec)
+{
+    if (!b || !spec) return kErrArg;
+    return (long long)static_cast<BatchBase *>(b)->bytes(*spec);
+}
+
+int hydro_batch_copy_state(void *b, int slot, void *rhoE, void *uvx, int to_host)
+{
+    if (!b || !rhoE || !uvx) return kErrArg;
+    return static_cast<BatchBase *>(b)->copy_state(slot, rhoE, uvx, to_host != 0);
+}
+
+void hydro_batch_destroy(void *b) { delete static_cast<BatchBase *>(b); }
+
+} // extern "C"

@@ -31,6 +31,7 @@
 
 #include "../../include/hydro_b200.h"
 #include "hydro_host.h"
+#include "strip2d_march.cuh"
 
 namespace hydro {
 
@@ -58,15 +59,6 @@ __device__ __forceinline__ float skip_threshold_f(const StepScratch *scr, unsign
     return __double2float_rd(skip_threshold(scr, key));
 }
 
-__device__ __forceinline__ int wrap_row(int n, int nb_x) { return n == 0 ? nb_x : (n == nb_x + 1 ? 1 : n); }
-
-template <class T> __device__ __forceinline__ typename Vec2<T>::type mk2(T a, T b)
-{
-    typename Vec2<T>::type v;
-    v.x = a;
-    v.y = b;
-    return v;
-}
 
 // ------------------------------------------------------------------ direct kernel ---
 constexpr int kDirectNT = 128;
@@ -121,132 +113,30 @@ template <class T> __global__ void __launch_bounds__(kRedoNT) redo2d(Args2<T> g)
 }
 
 // ------------------------------------------------------------------- strip kernel ---
-constexpr int kStripNT = 128;
-constexpr int kStripW = kStripNT - 2; // interior columns per strip
-constexpr int kStages = 4;
-
 template <class T>
 __global__ void __launch_bounds__(kStripNT, 4)
     strip2d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args2<T> g)
 {
-    using V2 = typename Vec2<T>::type;
-    constexpr unsigned FULL = 0xffffffffu;
-    constexpr uint32_t kStageBytes = 2u * kStripNT * sizeof(V2);
-    __shared__ __align__(128) V2 sr[kStages][kStripNT];
-    __shared__ __align__(128) V2 su[kStages][kStripNT];
-    __shared__ __align__(8) uint64_t full[kStages];
-    // y-face inputs of every lane's cell (lane t at [t]) and every lane's right face flux
-    // (lane t at [t+1]), stored as pairs so that each lane moves them with 128-bit
-    // (FP64) / 64-bit (FP32) shared-memory accesses
-    __shared__ __align__(16) V2 xP[4][kStripNT + 1];
-    __shared__ __align__(16) V2 xF[2][kStripNT + 1];
-    __shared__ int s_abort;
-
-    const int t = threadIdx.x;
-    const int jbase = kStripW * blockIdx.x; // column held by lane 0
-    const int j = jbase + t;
-    const int i0 = 1 + g.chunk * blockIdx.y;
-    const int i1 = min(i0 + g.chunk - 1, g.nb_x);
-    const int nrows = i1 - i0 + 3; // with one halo row above and below
-    const bool interior = (t >= 1) && (t <= kStripW) && (j <= g.nb_y);
-    const int xcoord = 2 * jbase;
-    // the two wall faces live in at most two warps; the others skip the mirror selects
-    const bool wall_warp = __any_sync(FULL, j == 0 || j == g.nb_y);
-
-    if (t == 0) {
+    __shared__ Smem2<T> S;
+    if (threadIdx.x == 0) {
         prefetch_tensormap(&tmr);
         prefetch_tensormap(&tmu);
-        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
-        fence_mbar_init();
-        s_abort = 0;
     }
-    __syncthreads();
-    auto issue = [&](int m) {
-        const int s = m % kStages;
-        const int row = wrap_row(i0 - 1 + m, g.nb_x);
-        mbar_arrive_expect_tx(&full[s], kStageBytes);
-        tma_load_2d(&sr[s][0], &tmr, xcoord, row, &full[s]);
-        tma_load_2d(&su[s][0], &tmu, xcoord, row, &full[s]);
-    };
-    if (t == 0)
-        for (int m = 0; m < kStages && m < nrows; ++m) issue(m);
-
+    march2d_init(S);
+    const int i0 = 1 + g.chunk * (int)blockIdx.y;
+    const March2 geo{kStripW * (int)blockIdx.x, i0, min(i0 + g.chunk - 1, g.nb_x), g.nb_x, g.nb_y, g.ys};
     StepAcc acc;
-    Cell2<T> Pm{};
-    T Ur = 0, Uu = 0, Uv = 0, UE = 0;
-    Flux2<T> fxlo{}, fyl{}, fyr{};
-    // lanes whose column is a ghost (j = 0, j = NB_Y+1) or past the array hold zeros;
-    // their primitives are never used, so they convert a unit state instead (keeps the
-    // reciprocal / square root of every lane on its regular path)
-    const bool real_col = (j >= 1) && (j <= g.nb_y);
     const float tlof = skip_threshold_f(g.scr, g.key);
-    int m = 0;
-#pragma unroll 2
-    for (; m < nrows; ++m) {
-        const int s = m % kStages;
-        if (!mbar_wait_bounded(&full[s], (m / kStages) & 1)) s_abort = 1;
-        V2 a = sr[s][t], b = su[s][t];
-        if (!real_col) {
-            a = mk2<T>(T(1), T(1));
-            b = mk2<T>(T(0), T(0));
-        }
-        const Cell2<T> P = make_cell2<T>(a.x, b.x, b.y, a.y, g.ph);
-        const bool yrow = (m >= 1) && (m <= nrows - 2);
-        if (yrow) {
-            const FaceIn<T> me = face_y(P);
-            xP[0][t] = mk2<T>(me.r, me.un);
-            xP[1][t] = mk2<T>(me.p, me.Ka);
-            xP[2][t] = mk2<T>(me.iKa, me.mn);
-            xP[3][t] = mk2<T>(me.mt, me.eup);
-        }
-        __syncthreads(); // stage s consumed by every lane; y-face inputs published
-        if (s_abort) break;
-        if (t == 0 && m + kStages < nrows) issue(m + kStages);
-
-        if (m >= 1) {
-            // x face (row n-1 | row n) of this column; then the update of row n-1
-            const Flux2<T> fxhi = face_flux(face_x(Pm), face_x(P), g.ph);
-            if (m >= 2 && interior) {
-                const Upd2<T> o = update2(Ur, Uu, Uv, UE, fxlo, fxhi, fyl, fyr, g.DtDx, g.DtDy, g.ph);
-                const long long c = (long long)(i0 + m - 2) * g.ys + j;
-                reinterpret_cast<V2 *>(g.rhoE_n)[c] = mk2<T>(o.r, o.E);
-                reinterpret_cast<V2 *>(g.uv_n)[c] = mk2<T>(o.u, o.v);
-                acc.add_mass(o.r);
-                const float fu = (float)o.u, fv = (float)o.v;
-                const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv, g.ggm1);
-                if (!(ub < tlof)) acc.add_speed(speed2(o.r, o.u, o.v, o.E, g.ph));
-            }
-            fxlo = fxhi;
-        }
-        if (yrow) {
-            // y face (j | j+1) of row n, from this lane's cell and the next lane's
-            const FaceIn<T> me = face_y(P);
-            const V2 n0 = xP[0][t + 1], n1 = xP[1][t + 1], n2 = xP[2][t + 1], n3 = xP[3][t + 1];
-            FaceIn<T> L = me;
-            FaceIn<T> R{n0.x, n0.y, n1.x, n1.y, n2.x, n2.y, n3.x, n3.y};
-            if (wall_warp) {
-                if (j == 0) L = mirror(R);       // wall at j = 1/2
-                if (j == g.nb_y) R = mirror(me); // wall at j = NB_Y + 1/2
-            }
-            fyr = face_flux(L, R, g.ph);
-            xF[0][t + 1] = mk2<T>(fyr.r, fyr.n);
-            xF[1][t + 1] = mk2<T>(fyr.t, fyr.E);
-            __syncthreads(); // right faces published: lane t's left face is lane t-1's right
-            const V2 f0 = xF[0][t], f1 = xF[1][t];
-            fyl = Flux2<T>{f0.x, f0.y, f1.x, f1.y};
-        }
-        Pm = P;
-        Ur = a.x; Uu = b.x; Uv = b.y; UE = a.y;
-    }
-    if (m < nrows) {
-        // gave up on a barrier: wait (bounded) for the loads still in flight before the
-        // block's shared memory is released, and report the time-out
-        acc.err |= kErrWaitTimeout;
-        if (t == 0)
-            for (int q = m; q < nrows && q < m + kStages; ++q)
-                (void)mbar_wait_bounded(&full[q % kStages], (q / kStages) & 1);
-        __syncthreads();
-    }
+    const float ggm1 = g.ggm1;
+    const Phys<T> ph = g.ph;
+    unsigned ld = 0;
+    const bool ok = march2d<T>(S, &tmr, &tmu, geo, g.rhoE_n, g.uv_n, ph, g.DtDx, g.DtDy, ld, [&](const Upd2<T> &o) {
+        acc.add_mass(o.r);
+        const float fu = (float)o.u, fv = (float)o.v;
+        const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1);
+        if (!(ub < tlof)) acc.add_speed(speed2(o.r, o.u, o.v, o.E, ph));
+    });
+    if (!ok) acc.err |= kErrWaitTimeout;
     step_epilogue<kStripNT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y, blockIdx.x + blockIdx.y * gridDim.x,
                                g.ph.C_min, g.Dt_next, g.status, g.seq, (double)tlof, g.key);
 }
@@ -487,26 +377,20 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
 }
 
 template <class T>
-int init2d(T *rhoE, T *uv, size_t nb_x, size_t nb_y, T u_in, T u_out, T p_in, T p_out, T C_min, T gamma,
-           T *min_dt, cudaStream_t stream)
+int init2d_at(T *rhoE, T *uv, size_t nb_x, size_t nb_y, double cx, double cy, double radius, T u_in, T u_out, T p_in,
+              T p_out, T C_min, T gamma, T *min_dt, cudaStream_t stream, unsigned long long *bits, long long ys)
 {
-    if (!rhoE || !uv || !min_dt || nb_x == 0 || nb_y == 0 || nb_x > (1u << 30) || nb_y > (1u << 30)) {
+    if (!rhoE || !uv || !min_dt || !bits || nb_x == 0 || nb_y == 0 || nb_x > (1u << 30) || nb_y > (1u << 30)) {
         set_error(kErrArg, "init2d: invalid argument");
         return kErrArg;
     }
-    int err;
-    DevCtx *ctx = ctx_current(&err);
-    if (!ctx) return err;
-    unsigned long long *bits = &ctx->scr->max_bits; // borrowed while no step is in flight
     const T big = T(1e20);
     const unsigned long long init = (unsigned long long)__builtin_bit_cast(long long, (double)big);
-    const double cx = double(nb_x + 1) / 2.0, cy = double(nb_y + 1) / 2.0;
-    const double radius = std::min(cx, cy) / 3;
     const T gm1 = gamma - T(1);
     cudaError_t e = cudaMemcpyAsync(bits, &init, sizeof init, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
         const int gx = (int)((nb_y + 127) / 128), gy = (int)std::min<size_t>(nb_x, 65535);
-        init2d_kernel<T><<<dim3(gx, gy), 128, 0, stream>>>(rhoE, uv, (int)nb_x, (int)nb_y, (long long)nb_y + 2, cx, cy,
+        init2d_kernel<T><<<dim3(gx, gy), 128, 0, stream>>>(rhoE, uv, (int)nb_x, (int)nb_y, ys > 0 ? ys : (long long)nb_y + 2, cx, cy,
                                                            radius, u_in, u_out, p_in, p_out, C_min, gamma, gm1, bits);
         e = cudaGetLastError();
     }
@@ -521,6 +405,21 @@ int init2d(T *rhoE, T *uv, size_t nb_x, size_t nb_y, T u_in, T u_out, T p_in, T 
     }
     *min_dt = (T)__builtin_bit_cast(double, (long long)res);
     return kOk;
+}
+
+template <class T>
+int init2d(T *rhoE, T *uv, size_t nb_x, size_t nb_y, T u_in, T u_out, T p_in, T p_out, T C_min, T gamma,
+           T *min_dt, cudaStream_t stream)
+{
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    // the reference's circle: centre ((NB_X+1)/2, (NB_Y+1)/2), radius min(cx, cy)/3
+    const double cx = double(nb_x + 1) / 2.0, cy = double(nb_y + 1) / 2.0;
+    const double radius = std::min(cx, cy) / 3;
+    // the scratch max word is borrowed while no step is in flight
+    return init2d_at<T>(rhoE, uv, nb_x, nb_y, cx, cy, radius, u_in, u_out, p_in, p_out, C_min, gamma, min_dt, stream,
+                        &ctx->scr->max_bits);
 }
 
 template <class T> int mass_sum(const T *rhoE, size_t nb_x, size_t nb_y, size_t nb_z, double *out, cudaStream_t s)
@@ -557,6 +456,10 @@ template int step2d<float>(const float *, const float *, float *, float *, float
                            size_t, float, float, cudaStream_t, Kernel, bool, StepInfo *);
 template int init2d<double>(double *, double *, size_t, size_t, double, double, double, double, double, double,
                             double *, cudaStream_t);
+template int init2d_at<double>(double *, double *, size_t, size_t, double, double, double, double, double, double,
+                               double, double, double, double *, cudaStream_t, unsigned long long *, long long);
+template int init2d_at<float>(float *, float *, size_t, size_t, double, double, double, float, float, float, float,
+                              float, float, float *, cudaStream_t, unsigned long long *, long long);
 template int init2d<float>(float *, float *, size_t, size_t, float, float, float, float, float, float, float *,
                            cudaStream_t);
 template int mass_sum<double>(const double *, size_t, size_t, size_t, double *, cudaStream_t);

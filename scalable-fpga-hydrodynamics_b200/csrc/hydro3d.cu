@@ -440,22 +440,17 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
 }
 
 template <class T>
-int init3d(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, T u_in, T u_out, T p_in, T p_out, T C_min,
-           T gamma, T *min_dt, cudaStream_t stream)
+int init3d_at(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, double cx, double cy, double cz, double radius,
+              T u_in, T u_out, T p_in, T p_out, T C_min, T gamma, T *min_dt, cudaStream_t stream,
+              unsigned long long *bits)
 {
-    if (!rhoE || !uvw || !min_dt || nb_x == 0 || nb_y == 0 || nb_z == 0 || nb_x > (1u << 30) ||
+    if (!rhoE || !uvw || !min_dt || !bits || nb_x == 0 || nb_y == 0 || nb_z == 0 || nb_x > (1u << 30) ||
         (nb_y + 3) / 4 > 65535) {
         set_error(kErrArg, "init3d: invalid argument");
         return kErrArg;
     }
-    int err;
-    DevCtx *ctx = ctx_current(&err);
-    if (!ctx) return err;
-    unsigned long long *bits = &ctx->scr->max_bits;
     const T big = T(1e20);
     const unsigned long long init = (unsigned long long)__builtin_bit_cast(long long, (double)big);
-    const double cx = double(nb_x + 1) / 2.0, cy = double(nb_y + 1) / 2.0, cz = double(nb_z + 1) / 2.0;
-    const double radius = std::min({cx, cy, cz}) / 3;
     const T gm1 = gamma - T(1);
     cudaError_t e = cudaMemcpyAsync(bits, &init, sizeof init, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
@@ -478,6 +473,25 @@ int init3d(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, T u_in, T u_o
     *min_dt = (T)__builtin_bit_cast(double, (long long)res);
     return kOk;
 }
+
+template <class T>
+int init3d(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, T u_in, T u_out, T p_in, T p_out, T C_min,
+           T gamma, T *min_dt, cudaStream_t stream)
+{
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    // the reference's sphere: centre ((N+1)/2 per axis), radius min(centres)/3
+    const double cx = double(nb_x + 1) / 2.0, cy = double(nb_y + 1) / 2.0, cz = double(nb_z + 1) / 2.0;
+    const double radius = std::min({cx, cy, cz}) / 3;
+    return init3d_at<T>(rhoE, uvw, nb_x, nb_y, nb_z, cx, cy, cz, radius, u_in, u_out, p_in, p_out, C_min, gamma,
+                        min_dt, stream, &ctx->scr->max_bits);
+}
+
+template int init3d_at<double>(double *, double *, size_t, size_t, size_t, double, double, double, double, double,
+                               double, double, double, double, double, double *, cudaStream_t, unsigned long long *);
+template int init3d_at<float>(float *, float *, size_t, size_t, size_t, double, double, double, double, float, float,
+                              float, float, float, float, float *, cudaStream_t, unsigned long long *);
 
 template int step3d<double>(const double *, const double *, double *, double *, double *, const Phys<double> &,
                             size_t, size_t, size_t, double, double, double, cudaStream_t, Kernel, bool, StepInfo *);

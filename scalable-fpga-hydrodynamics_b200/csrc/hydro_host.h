@@ -119,6 +119,17 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
 template <class T>
 int init2d(T *rhoE, T *uv, size_t nb_x, size_t nb_y, T u_in, T u_out, T p_in, T p_out, T C_min, T gamma,
            T *min_dt, cudaStream_t stream);
+// The same blast with an explicit centre (cx, cy) and radius in cell-index units (the
+// reference's coordinates: interior cells are 1..NB), densities rho_in/rho_out and
+// pressures p_in/p_out. `bits` is one device word of scratch; `ys` the row stride in
+// cells (0: NB_Y + 2, the reference layout).
+template <class T>
+int init2d_at(T *rhoE, T *uv, size_t nb_x, size_t nb_y, double cx, double cy, double radius, T u_in, T u_out, T p_in,
+              T p_out, T C_min, T gamma, T *min_dt, cudaStream_t stream, unsigned long long *bits, long long ys = 0);
+template <class T>
+int init3d_at(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, double cx, double cy, double cz, double radius,
+              T u_in, T u_out, T p_in, T p_out, T C_min, T gamma, T *min_dt, cudaStream_t stream,
+              unsigned long long *bits);
 template <class T>
 int init3d(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, T u_in, T u_out, T p_in, T p_out, T C_min,
            T gamma, T *min_dt, cudaStream_t stream);

@@ -1,0 +1,166 @@
+// The row march of the 2D strip kernels, shared by the plain step (strip2d, one
+// strip x chunk per block) and the batched step (batch2d, many strips x chunks of many
+// instances per persistent block).
+//
+// One block of kStripNT lanes covers kStripNT consecutive columns starting at `jbase`
+// (kStripW interior columns plus a halo column each side) and marches over rows
+// i0-1 .. i1+1. Each row of each array arrives in shared memory by one TMA tile load
+// into a kStages-deep ring of mbarrier-tracked stages; `ld` counts the loads this
+// block has issued so far, so consecutive marches of one block reuse the ring without
+// re-initialising the barriers. Every updated interior cell is handed to `sink`.
+#pragma once
+
+#include "hydro_rt.cuh"
+
+namespace hydro {
+
+constexpr int kStripNT = 128;
+constexpr int kStripW = kStripNT - 2; // interior columns per strip
+constexpr int kStages = 4;
+
+__device__ __forceinline__ int wrap_row(int n, int nb_x) { return n == 0 ? nb_x : (n == nb_x + 1 ? 1 : n); }
+
+template <class T> __device__ __forceinline__ typename Vec2<T>::type mk2(T a, T b)
+{
+    typename Vec2<T>::type v;
+    v.x = a;
+    v.y = b;
+    return v;
+}
+
+template <class T> struct Smem2 {
+    using V2 = typename Vec2<T>::type;
+    __align__(128) V2 sr[kStages][kStripNT]; // (rho, E) rows
+    __align__(128) V2 su[kStages][kStripNT]; // (rho u, rho v) rows
+    // y-face inputs of every lane's cell (lane t at [t]) and every lane's right face
+    // flux (lane t at [t+1]), as pairs so that each lane moves them with 128-bit (FP64)
+    // or 64-bit (FP32) shared-memory accesses
+    __align__(16) V2 xP[4][kStripNT + 1];
+    __align__(16) V2 xF[2][kStripNT + 1];
+    __align__(8) uint64_t full[kStages];
+    int abort;
+};
+
+// One-time set-up of the stage barriers (thread 0), followed by a block barrier.
+template <class T> __device__ __forceinline__ void march2d_init(Smem2<T> &S)
+{
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&S.full[s], 1);
+        fence_mbar_init();
+        S.abort = 0;
+    }
+    __syncthreads();
+}
+
+struct March2 {
+    int jbase, i0, i1; // columns jbase .. jbase+kStripNT-1, interior rows i0 .. i1
+    int nb_x, nb_y;
+    long long ys;
+};
+
+// Returns false when a bounded barrier wait gave up (the block then stops marching).
+template <class T, class Sink>
+__device__ __forceinline__ bool march2d(Smem2<T> &S, const CUtensorMap *tmr, const CUtensorMap *tmu, const March2 &g,
+                                        T *rhoE_n, T *uv_n, const Phys<T> &ph, T DtDx, T DtDy, unsigned &ld,
+                                        Sink &&sink)
+{
+    using V2 = typename Vec2<T>::type;
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr uint32_t kStageBytes = 2u * kStripNT * sizeof(V2);
+    const int t = threadIdx.x;
+    const int j = g.jbase + t;
+    const int nrows = g.i1 - g.i0 + 3; // with one halo row above and below
+    const bool interior = (t >= 1) && (t <= kStripW) && (j <= g.nb_y);
+    const int xcoord = 2 * g.jbase;
+    // the two wall faces live in at most two warps; the others skip the mirror selects
+    const bool wall_warp = __any_sync(FULL, j == 0 || j == g.nb_y);
+    // lanes whose column is a ghost (j = 0, j = NB_Y+1) or past the array hold zeros;
+    // their primitives are never used, so they convert a unit state instead (keeps the
+    // reciprocal / square root of every lane on its regular path)
+    const bool real_col = (j >= 1) && (j <= g.nb_y);
+    const unsigned ld0 = ld;
+
+    auto issue = [&](int m) {
+        const unsigned q = ld0 + (unsigned)m;
+        const int s = q % kStages;
+        const int row = wrap_row(g.i0 - 1 + m, g.nb_x);
+        mbar_arrive_expect_tx(&S.full[s], kStageBytes);
+        tma_load_2d(&S.sr[s][0], tmr, xcoord, row, &S.full[s]);
+        tma_load_2d(&S.su[s][0], tmu, xcoord, row, &S.full[s]);
+    };
+    if (t == 0)
+        for (int m = 0; m < kStages && m < nrows; ++m) issue(m);
+
+    Cell2<T> Pm{};
+    T Ur = 0, Uu = 0, Uv = 0, UE = 0;
+    Flux2<T> fxlo{}, fyl{}, fyr{};
+    int m = 0;
+#pragma unroll 2
+    for (; m < nrows; ++m) {
+        const unsigned q = ld0 + (unsigned)m;
+        const int s = q % kStages;
+        if (!mbar_wait_bounded(&S.full[s], (q / kStages) & 1)) S.abort = 1;
+        V2 a = S.sr[s][t], b = S.su[s][t];
+        if (!real_col) {
+            a = mk2<T>(T(1), T(1));
+            b = mk2<T>(T(0), T(0));
+        }
+        const Cell2<T> P = make_cell2<T>(a.x, b.x, b.y, a.y, ph);
+        const bool yrow = (m >= 1) && (m <= nrows - 2);
+        if (yrow) {
+            const FaceIn<T> me = face_y(P);
+            S.xP[0][t] = mk2<T>(me.r, me.un);
+            S.xP[1][t] = mk2<T>(me.p, me.Ka);
+            S.xP[2][t] = mk2<T>(me.iKa, me.mn);
+            S.xP[3][t] = mk2<T>(me.mt, me.eup);
+        }
+        __syncthreads(); // stage s consumed by every lane; y-face inputs published
+        if (S.abort) break;
+        if (t == 0 && m + kStages < nrows) issue(m + kStages);
+
+        if (m >= 1) {
+            // x face (row n-1 | row n) of this column; then the update of row n-1
+            const Flux2<T> fxhi = face_flux(face_x(Pm), face_x(P), ph);
+            if (m >= 2 && interior) {
+                const Upd2<T> o = update2(Ur, Uu, Uv, UE, fxlo, fxhi, fyl, fyr, DtDx, DtDy, ph);
+                const long long c = (long long)(g.i0 + m - 2) * g.ys + j;
+                reinterpret_cast<V2 *>(rhoE_n)[c] = mk2<T>(o.r, o.E);
+                reinterpret_cast<V2 *>(uv_n)[c] = mk2<T>(o.u, o.v);
+                sink(o);
+            }
+            fxlo = fxhi;
+        }
+        if (yrow) {
+            // y face (j | j+1) of row n, from this lane's cell and the next lane's
+            const FaceIn<T> me = face_y(P);
+            const V2 n0 = S.xP[0][t + 1], n1 = S.xP[1][t + 1], n2 = S.xP[2][t + 1], n3 = S.xP[3][t + 1];
+            FaceIn<T> L = me;
+            FaceIn<T> R{n0.x, n0.y, n1.x, n1.y, n2.x, n2.y, n3.x, n3.y};
+            if (wall_warp) {
+                if (j == 0) L = mirror(R);       // wall at j = 1/2
+                if (j == g.nb_y) R = mirror(me); // wall at j = NB_Y + 1/2
+            }
+            fyr = face_flux(L, R, ph);
+            S.xF[0][t + 1] = mk2<T>(fyr.r, fyr.n);
+            S.xF[1][t + 1] = mk2<T>(fyr.t, fyr.E);
+            __syncthreads(); // right faces published: lane t's left face is lane t-1's right
+            const V2 f0 = S.xF[0][t], f1 = S.xF[1][t];
+            fyl = Flux2<T>{f0.x, f0.y, f1.x, f1.y};
+        }
+        Pm = P;
+        Ur = a.x; Uu = b.x; Uv = b.y; UE = a.y;
+    }
+    ld = ld0 + (unsigned)nrows;
+    if (m < nrows) {
+        // gave up on a barrier: wait (bounded) for the loads still in flight before the
+        // block's shared memory is released
+        if (t == 0)
+            for (int q = m; q < nrows && q < m + kStages; ++q)
+                (void)mbar_wait_bounded(&S.full[(ld0 + q) % kStages], ((ld0 + q) / kStages) & 1);
+        __syncthreads();
+        return false;
+    }
+    return true;
+}
+
+} // namespace hydro

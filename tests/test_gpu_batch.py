@@ -1,0 +1,111 @@
+"""Batched step: bit-identical to the plain path per instance, independent of the mix,
+FP32 within the stated tolerance of the FP64 oracle, conservation sums reported."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_pkg
+
+hb = load_pkg()
+pytestmark = pytest.mark.gpu
+
+
+def interior(st, nb):
+    import oracle as orc
+
+    return orc.interior(st, nb)
+
+
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+def test_batch_instance_equals_plain_path(cuda, T):
+    """The reference blast through the batch (with other instances around it) and through
+    the plain path: same Dt sequence end, same t, same interior bits."""
+    from hydro_b200.batch import Batch, Blast
+
+    nb = (300, 250) if T is np.float64 else (300, 252)
+    steps = 40
+    plain = hb.BlastRun(nb, T).run(1e9, steps)
+    b = Batch(2, T, capacity=8)
+    others = [b.add(Blast(nb=(97, 131), max_steps=steps + 5)), b.add(Blast(nb=(64, 500), max_steps=3))]
+    slot = b.add(Blast(nb=nb, max_steps=steps))
+    b.run(steps + 5)
+    st = b.status(slot)
+    assert st["steps"] == steps and not st["active"]
+    assert st["t"] == plain.t
+    assert np.float64(st["dt"]) == np.float64(plain.dt)
+    ours = interior(b.state(slot), nb)
+    ref = interior(plain.host_state(), nb)
+    assert ours[0].tobytes() == ref[0].tobytes() and ours[1].tobytes() == ref[1].tobytes()
+    assert abs(st["mass"] - plain.mass()) <= 1e-13 * st["mass"]
+    assert b.status(others[1])["steps"] == 3
+    b.close()
+
+
+def test_batch_result_independent_of_mix(cuda):
+    """Each instance alone and in a mix of 24 uneven instances: identical bits, identical
+    conservation sums (the per-instance reduction order does not depend on the mix)."""
+    from hydro_b200.batch import Batch
+    from hydro_b200.workloads import batch_blasts
+
+    blasts = batch_blasts(24, seed=3, steps=30)
+    for bl in blasts:  # keep the test quick: shrink the largest instances
+        bl.nb = tuple(min(n, 400) for n in bl.nb)
+        bl.centre = tuple(min(c, n) for c, n in zip(bl.centre, bl.nb))
+        bl.radius = min(bl.radius, 0.2 * min(bl.nb))
+    mix = Batch(2, np.float32, capacity=64)
+    slots = [mix.add(bl) for bl in blasts]
+    mix.run(30)
+    for k in (0, 7, 23):
+        alone = Batch(2, np.float32, capacity=4)
+        s = alone.add(blasts[k])
+        alone.run(30)
+        a, m = alone.status(s), mix.status(slots[k])
+        assert a == m, (k, a, m)
+        sa, sm = alone.state(s), mix.state(slots[k])
+        assert sa[0].tobytes() == sm[0].tobytes() and sa[1].tobytes() == sm[1].tobytes()
+        alone.close()
+    mix.close()
+
+
+def test_batch_fp32_accuracy_vs_fp64_oracle(cuda, oracle):
+    """The reference 60x60 blast through the FP32 batch against the FP64 oracle after
+    200 steps: relative L1 on rho <= 1e-5."""
+    from hydro_b200.batch import Batch, Blast
+
+    nb = (60, 60)
+    r64 = oracle.run(nb, np.float64, 2.0, 200)
+    b = Batch(2, np.float32, capacity=2)
+    s = b.add(Blast(nb=nb, t_end=2.0, max_steps=200))
+    b.run(200)
+    st = b.status(s)
+    assert st["steps"] == r64["it"]
+    a = interior(b.state(s), nb)[0][..., 0].astype(np.float64)
+    r = interior(r64["state"], nb)[0][..., 0]
+    l1 = np.abs(a - r).sum() / np.abs(r).sum()
+    linf = np.abs(a - r).max() / np.abs(r).max()
+    print(f"batched FP32 vs FP64 oracle: rho rel L1 {l1:.2e}, rel Linf {linf:.2e}")
+    assert l1 <= 1e-5
+    assert abs(st["mass"] - r64["mass1"]) <= 1e-5 * r64["mass1"]
+    b.close()
+
+
+def test_batch_retire_remove_reuse(cuda):
+    """Instances retire at t_end, slots are reused, the graph is rebuilt on change."""
+    from hydro_b200.batch import Batch, Blast
+
+    b = Batch(2, np.float32, capacity=2)
+    s0 = b.add(Blast(nb=(64, 64), t_end=0.01))
+    s1 = b.add(Blast(nb=(80, 48), max_steps=10))
+    b.run(50)
+    st0, st1 = b.status(s0), b.status(s1)
+    assert not st0["active"] and st0["t"] >= 0.01 and st0["steps"] < 50
+    assert st1["steps"] == 10
+    b.remove(s0)
+    s2 = b.add(Blast(nb=(70, 70), max_steps=5))
+    assert s2 == s0
+    b.run(10)
+    assert b.status(s2)["steps"] == 5
+    with pytest.raises(hb.HydroError):
+        b.add(Blast(nb=(10, 10)))  # both slots in use
+    b.close()
