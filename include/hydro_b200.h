@@ -213,7 +213,25 @@ int hydro_batch_state(void *batch, int slot, const void **rhoE, const void **uvx
 /* Copy an instance's current state into caller buffers in the reference layout
  * ((NB_X+2)(NB_Y+2) cells, no row padding); `to_host` selects host or device buffers. */
 int hydro_batch_copy_state(void *batch, int slot, void *rhoE, void *uvx, int to_host);
+/* Wait for every step enqueued on the batch. */
+int hydro_batch_sync(void *batch);
 void hydro_batch_destroy(void *batch);
+
+/* The blast initial condition of hydro2d/main.cxx:280-338 (hydro3d/main.cxx:296-363) with
+ * an explicit centre and radius (cell-index units) and densities/pressures inside and
+ * outside, for the plain path; first Dt in *min_dt (host). Synchronous. */
+int hydro2d_init_blast_at_f64(double *d_rhoE, double *d_uv, size_t NB_X, size_t NB_Y, double cx, double cy,
+                              double radius, double rho_in, double rho_out, double p_in, double p_out, double C_min,
+                              double gamma, double *min_dt, void *stream);
+int hydro2d_init_blast_at_f32(float *d_rhoE, float *d_uv, size_t NB_X, size_t NB_Y, double cx, double cy,
+                              double radius, float rho_in, float rho_out, float p_in, float p_out, float C_min,
+                              float gamma, float *min_dt, void *stream);
+int hydro3d_init_blast_at_f64(double *d_rhoE, double *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, double cx,
+                              double cy, double cz, double radius, double rho_in, double rho_out, double p_in,
+                              double p_out, double C_min, double gamma, double *min_dt, void *stream);
+int hydro3d_init_blast_at_f32(float *d_rhoE, float *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, double cx,
+                              double cy, double cz, double radius, float rho_in, float rho_out, float p_in,
+                              float p_out, float C_min, float gamma, float *min_dt, void *stream);
 
 /* ---- errors -------------------------------------------------------------------------- */
 /* No counterpart in the reference (it has no status return): last error code latched

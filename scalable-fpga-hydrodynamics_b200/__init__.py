@@ -136,6 +136,14 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+class _nullctx:
+    def __enter__(self):
+        return None
+
+    def __exit__(self, *a):
+        return False
+
+
 # --------------------------------------------------------------------------- physics ---
 @dataclass
 class Physics:
@@ -241,6 +249,25 @@ def init_blast(state, phys: Physics, rho_in=1.0, rho_out=1.2, p_in=10.0, p_out=0
     return T(out.value)
 
 
+def init_blast_at(state, phys: Physics, blast, stream=None):
+    """Device blast IC with the explicit centre/radius/densities of a `Blast`; first Dt."""
+    L = lib()
+    T = phys.dtype
+    f64 = T is np.float64
+    CT = ctypes.c_double if f64 else ctypes.c_float
+    suf = "f64" if f64 else "f32"
+    fn = getattr(L, f"hydro{len(phys.nb)}d_init_blast_at_{suf}")
+    d = ctypes.c_double
+    nd = len(phys.nb)
+    fn.argtypes = [_vp, _vp] + [_c_size] * nd + [d] * (nd + 1) + [CT] * 6 + [ctypes.POINTER(CT), _vp]
+    fn.restype = ctypes.c_int
+    out = CT(0)
+    _check(fn(_ptr(state[0]), _ptr(state[1]), *phys.nb, *[float(c) for c in blast.centre[:nd]], float(blast.radius),
+              T(blast.rho_in), T(blast.rho_out), T(blast.p_in), T(blast.p_out), phys.C_min, phys.g,
+              ctypes.byref(out), _stream_handle(stream)))
+    return T(out.value)
+
+
 def mass(rhoE, nb, stream=None) -> float:
     """Compensated FP64 sum of the interior density (device)."""
     L = lib()
@@ -268,18 +295,27 @@ class BlastRun:
     (hydro2d/main.cxx:686-815): state stays on the device; each step reads the new Dt
     back (the only per-step device-to-host copy the loop needs)."""
 
-    def __init__(self, nb, dtype=np.float64, kernel=KERNEL_AUTO, stream=None):
+    def __init__(self, nb, dtype=np.float64, kernel=KERNEL_AUTO, stream=None, blast=None):
+        """`blast` (a hydro_b200.batch.Blast) overrides the reference's initial condition
+        and constants with an explicit centre, radius, densities, pressures, gamma, K, C."""
         torch = _torch()
         self.nb = tuple(int(n) for n in nb)
         self.T = dtype
-        self.phys = Physics(dtype, self.nb)
+        if blast is None:
+            self.phys = Physics(dtype, self.nb)
+        else:
+            self.phys = Physics(dtype, self.nb, C=blast.C, gamma=blast.gamma, K=blast.K)
         self.kernel = kernel
         self.stream = stream
-        self.cur = alloc_state(self.nb, dtype)
-        self.nxt = alloc_state(self.nb, dtype)
+        with torch.cuda.stream(stream) if stream is not None else _nullctx():
+            self.cur = alloc_state(self.nb, dtype)
+            self.nxt = alloc_state(self.nb, dtype)
         tdt = torch.float64 if dtype is np.float64 else torch.float32
         self.dt_dev = torch.zeros(1, dtype=tdt, device="cuda")
-        self.first_dt = init_blast(self.cur, self.phys, stream=stream)
+        if blast is None:
+            self.first_dt = init_blast(self.cur, self.phys, stream=stream)
+        else:
+            self.first_dt = init_blast_at(self.cur, self.phys, blast, stream=stream)
         big = dtype(1e20)
         self.dt = self.first_dt if not (big < self.first_dt) else big
         self.t = 0.0

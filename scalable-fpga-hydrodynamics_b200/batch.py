@@ -90,6 +90,8 @@ def _declare(L):
     L.hydro_batch_copy_state.restype = _c.c_int
     L.hydro_batch_destroy.argtypes = [vp]
     L.hydro_batch_destroy.restype = None
+    L.hydro_batch_sync.argtypes = [vp]
+    L.hydro_batch_sync.restype = _c.c_int
     L._batch_declared = True
     return L
 
@@ -135,6 +137,9 @@ class Batch:
 
     def run(self, nsteps: int, sync: bool = True):
         _check(self.L.hydro_batch_run(self.h, nsteps, 1 if sync else 0))
+
+    def sync(self):
+        _check(self.L.hydro_batch_sync(self.h))
 
     def status(self, slot: int) -> dict:
         s = BatchStatus()

@@ -1,23 +1,24 @@
-// Batched step: many independent 2D blast instances of uneven sizes advanced by one
-// persistent kernel per step, each instance with its own time step, boundaries and
+// Batched step: many independent 2D or 3D blast instances of uneven sizes advanced by
+// one persistent kernel per step, each instance with its own time step, boundaries and
 // simulated time (the layered "batching" change of the plain path; no counterpart in the
 // reference, whose host loop advances one domain, hydro2d/main.cxx:689-815).
 //
-// Each instance keeps the plain path's layout (two interleaved-pair arrays with ghosts,
-// double-buffered) and the plain path's arithmetic: the same strip march
-// (strip2d_march.cuh), so an instance's state after n batched steps is bit-identical to n
-// plain steps. Work is a flat list of (instance, strip x chunk) items; persistent blocks
-// take items from an atomic counter. Every item writes its partial sums (compensated FP64
-// mass, momenta and energy; max signal speed; error bits) to its own slot; the item that
-// completes an instance's step (ticket per instance) merges that instance's slots in
-// item order -- the result does not depend on which block ran which item, nor on the
-// other instances in the batch -- and advances the instance on the device:
+// Each instance keeps the plain path's arithmetic: the same strip march
+// (strip2d_march.cuh / strip3d_march.cuh), so an instance's state after n batched steps
+// is bit-identical to n plain steps in the same precision. 2D instances keep the pair
+// layout with rows padded to 16 bytes (TMA-fed); 3D instances keep the reference's
+// pair/triple layout (cp.async-fed). Work is a flat list of (instance, tile x chunk)
+// items; persistent blocks take items from an atomic counter. Every item writes its
+// partial sums (compensated FP64 mass, momenta and energy; max signal speed; error bits)
+// to its own slot; the item that completes an instance's step (ticket per instance)
+// merges that instance's slots in item order -- the result depends neither on which
+// block ran which item nor on the other instances in the batch -- and advances the
+// instance on the device:
 //   Dt = min(1e20, C_min / max_speed)   (hydro2d/kernel.cxx:318, main.cxx:706-781)
-//   t += Dt (FP64 accumulator), DtDx = Dt / DX, DtDy = Dt / DY (main.cxx:703-704, in T)
+//   t += Dt (FP64 accumulator), DtDx = Dt / DX ... (main.cxx:703-704, in T)
 //   active while t < t_end and steps < max_steps (main.cxx:689)
 // so a step needs no host round trip and n steps are captured as one CUDA graph.
 #include <algorithm>
-#include <mutex>
 #include <stdio.h>
 #include <string.h>
 #include <vector>
@@ -25,6 +26,7 @@
 #include "../../include/hydro_b200.h"
 #include "hydro_host.h"
 #include "strip2d_march.cuh"
+#include "strip3d_march.cuh"
 
 namespace hydro {
 
@@ -39,6 +41,18 @@ template <class T> struct alignas(128) Inst2 {
     long long ys;
     long long steps, max_steps;
     int nb_x, nb_y, nstrips, chunk;
+    int parity, active;
+    unsigned done_items, err;
+};
+
+template <class T> struct alignas(128) Inst3 {
+    T *rhoE[2], *uvw[2];
+    Phys<T> ph;
+    T DX, DY, DZ, dt, DtDx, DtDy, DtDz;
+    double t, t_end;
+    long long zs, zy;
+    long long steps, max_steps;
+    int nb_x, nb_y, nb_z, ntz, nty, chunk;
     int parity, active;
     unsigned done_items, err;
 };
@@ -137,9 +151,41 @@ template <int NT> __device__ __forceinline__ void block_reduce(BatchAcc &a)
     __syncthreads();
 }
 
+template <class T> __device__ __forceinline__ void set_dtdz(Inst2<T> *, T) {}
+template <class T> __device__ __forceinline__ void set_dtdz(Inst3<T> *in, T Dt) { in->DtDz = Ar<T>::div(Dt, in->DZ); }
+
+// Time-step bookkeeping of one instance after its step (thread 0 of the finalising block).
+template <class T, class I> __device__ __forceinline__ void advance(I *in, const BatchAcc &a, SlotStatus *st)
+{
+    using A = Ar<T>;
+    const T big = T(1e20);
+    const T dtn = A::div(in->ph.C_min, static_cast<T>(a.vmax));
+    const T Dt = (dtn < big) ? dtn : big;
+    in->steps += 1;
+    in->t = __dadd_rn(in->t, (double)Dt);
+    in->dt = Dt;
+    in->DtDx = A::div(Dt, in->DX);
+    in->DtDy = A::div(Dt, in->DY);
+    set_dtdz<T>(in, Dt);
+    in->parity ^= 1;
+    in->err |= a.err;
+    in->active = (in->t < in->t_end) && (in->steps < in->max_steps) && !(in->err & kErrNonPhysical);
+    if (st) {
+        st->t = in->t;
+        st->dt = (double)Dt;
+        for (int q = 0; q < kSums; ++q) st->sums[q] = __dadd_rn(a.s[q], a.c[q]);
+        st->max_speed = a.vmax;
+        st->steps = in->steps;
+        st->active = in->active;
+        st->err = in->err;
+    }
+    __threadfence();
+    in->done_items = 0;
+}
+
 // Merge an instance's item slots in item order and advance the instance (whole block).
-template <int NT, class T>
-__device__ void finalize_instance(Inst2<T> *I, const ItemPart *parts, int nitems, SlotStatus *st)
+template <int NT, class T, class I>
+__device__ void finalize_instance(I *in, const ItemPart *parts, int nitems, SlotStatus *st)
 {
     BatchAcc a;
     unsigned long long mb = 0ull;
@@ -152,31 +198,31 @@ __device__ void finalize_instance(Inst2<T> *I, const ItemPart *parts, int nitems
     }
     a.vmax = __longlong_as_double((long long)mb);
     block_reduce<NT>(a);
+    if (threadIdx.x == 0) advance<T>(in, a, st);
+}
+
+// The item's partial sums into its slot; returns (in every thread) whether this item
+// completed its instance's step.
+template <int NT>
+__device__ __forceinline__ bool publish_item(BatchAcc &acc, ItemPart *parts, int w, unsigned *done, int nitems,
+                                             int *s_last)
+{
+    block_reduce<NT>(acc);
     if (threadIdx.x == 0) {
-        using A = Ar<T>;
-        const T big = T(1e20);
-        const T dtn = A::div(I->ph.C_min, static_cast<T>(a.vmax));
-        const T Dt = (dtn < big) ? dtn : big;
-        I->steps += 1;
-        I->t = __dadd_rn(I->t, (double)Dt);
-        I->dt = Dt;
-        I->DtDx = A::div(Dt, I->DX);
-        I->DtDy = A::div(Dt, I->DY);
-        I->parity ^= 1;
-        I->err |= a.err;
-        I->active = (I->t < I->t_end) && (I->steps < I->max_steps) && !(I->err & kErrNonPhysical);
-        if (st) {
-            st->t = I->t;
-            st->dt = (double)Dt;
-            for (int q = 0; q < kSums; ++q) st->sums[q] = __dadd_rn(a.s[q], a.c[q]);
-            st->max_speed = a.vmax;
-            st->steps = I->steps;
-            st->active = I->active;
-            st->err = I->err;
+        ItemPart &p = parts[w];
+        for (int q = 0; q < kSums; ++q) {
+            p.s[q] = acc.s[q];
+            p.c[q] = acc.c[q];
         }
+        p.maxbits = (unsigned long long)__double_as_longlong(acc.vmax);
+        p.err = acc.err;
         __threadfence();
-        I->done_items = 0;
+        *s_last = (atomicAdd(done, 1u) == (unsigned)nitems - 1u);
     }
+    __syncthreads();
+    const bool last = *s_last != 0;
+    if (last) __threadfence();
+    return last;
 }
 
 template <class T>
@@ -213,25 +259,45 @@ __global__ void __launch_bounds__(kStripNT, 4) batch2d(Inst2<T> *insts, const in
                                        acc.add(o.r, o.u, o.v, T(0), o.E, speed2(o.r, o.u, o.v, o.E, ph));
                                    });
         if (!ok) acc.err |= kErrWaitTimeout;
-        block_reduce<kStripNT>(acc);
-        if (threadIdx.x == 0) {
-            ItemPart &p = parts[w];
-            for (int q = 0; q < kSums; ++q) {
-                p.s[q] = acc.s[q];
-                p.c[q] = acc.c[q];
-            }
-            p.maxbits = (unsigned long long)__double_as_longlong(acc.vmax);
-            p.err = acc.err;
-            __threadfence();
-            const int2 rg = ranges[it.x];
-            s_last = (atomicAdd(&I->done_items, 1u) == (unsigned)rg.y - 1u);
-        }
-        __syncthreads();
-        if (s_last) {
-            __threadfence();
-            const int2 rg = ranges[it.x];
+        const int2 rg = ranges[it.x];
+        if (publish_item<kStripNT>(acc, parts, w, &I->done_items, rg.y, &s_last))
             finalize_instance<kStripNT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr);
-        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *items, const int2 *ranges,
+                                                  int nitems, unsigned *counter, ItemPart *parts,
+                                                  SlotStatus *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem3<T> &S = *reinterpret_cast<Smem3<T> *>(smem_raw);
+    __shared__ int s_item;
+    __shared__ int s_last;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int w = s_item;
+        if (w >= nitems) break;
+        const int2 it = items[w];
+        Inst3<T> *I = insts + it.x;
+        if (!I->active) continue;
+        const int par = I->parity;
+        const int tz = it.y % I->ntz, rem = it.y / I->ntz;
+        const int ty = rem % I->nty, ck = rem / I->nty;
+        const int i0 = 1 + ck * I->chunk;
+        const March3 geo{k3TZ * tz, k3TY * ty, i0, min(i0 + I->chunk - 1, I->nb_x), I->nb_x, I->nb_y, I->nb_z,
+                         I->zs, I->zy};
+        const Phys<T> ph = I->ph;
+        BatchAcc acc;
+        march3d<T>(S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy,
+                   I->DtDz, [&](const Upd3<T> &o) {
+                       acc.add(o.r, o.u, o.v, o.w, o.E, speed3(o.r, o.u, o.v, o.w, o.E, ph));
+                   });
+        const int2 rg = ranges[it.x];
+        if (publish_item<k3NT>(acc, parts, w, &I->done_items, rg.y, &s_last))
+            finalize_instance<k3NT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr);
     }
 }
 
@@ -246,17 +312,21 @@ class BatchBase {
     virtual int state(int slot, const void **rhoE, const void **uvx, long long *row_stride) = 0;
     virtual size_t bytes(const hydro_blast_t &spec) const = 0;
     virtual int copy_state(int slot, void *rhoE, void *uvx, bool to_host) = 0;
+    virtual int sync() = 0;
 };
 
-template <class T> class Batch2 final : public BatchBase {
+template <class T, int D> class BatchEngine final : public BatchBase {
+    using Inst = typename std::conditional<D == 2, Inst2<T>, Inst3<T>>::type;
+
   public:
-    Batch2(int chunk, int capacity, cudaStream_t stream, int *rc) : chunk_(chunk > 0 ? chunk : 128), cap_(capacity)
+    BatchEngine(int chunk, int capacity, cudaStream_t stream, int *rc)
+        : chunk_(chunk > 0 ? chunk : (D == 2 ? 128 : 64)), cap_(capacity)
     {
         own_stream_ = (stream == nullptr);
         cudaError_t e = cudaSuccess;
         if (own_stream_) e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
         else stream_ = stream;
-        if (e == cudaSuccess) e = cudaMalloc(&insts_, sizeof(Inst2<T>) * cap_);
+        if (e == cudaSuccess) e = cudaMalloc(&insts_, sizeof(Inst) * cap_);
         if (e == cudaSuccess) e = cudaMalloc(&ranges_, sizeof(int2) * cap_);
         if (e == cudaSuccess) e = cudaMalloc(&counter_, 64);
         if (e == cudaSuccess) e = cudaMalloc(&scratch_bits_, 64);
@@ -264,10 +334,17 @@ template <class T> class Batch2 final : public BatchBase {
         if (e == cudaSuccess) e = cudaHostAlloc(&status_h_, sizeof(SlotStatus) * cap_, cudaHostAllocMapped);
         if (e == cudaSuccess) e = cudaHostGetDevicePointer(&status_d_, status_h_, 0);
         if (e == cudaSuccess) memset(status_h_, 0, sizeof(SlotStatus) * cap_);
-        int dev = 0, nsm = 148, occ = 4;
+        int dev = 0, nsm = 148, occ = 1;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch2d<T>, kStripNT, 0);
+        if constexpr (D == 2) {
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch2d<T>, kStripNT, 0);
+        } else {
+            smem_ = (int)sizeof(Smem3<T>);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(batch3d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch3d<T>, k3NT, smem_);
+        }
         blocks_ = nsm * std::max(1, occ);
         slots_.resize(cap_);
         host_ranges_.assign(cap_, make_int2(0, 0));
@@ -275,11 +352,12 @@ template <class T> class Batch2 final : public BatchBase {
         if (e != cudaSuccess) set_error(kErrCuda, "batch create: %s", cudaGetErrorString(e));
     }
 
-    ~Batch2() override
+    ~BatchEngine() override
     {
         if (graph_) cudaGraphExecDestroy(graph_);
         for (auto &s : slots_)
             if (s.used) free_slot(s);
+        cudaStreamSynchronize(stream_);
         cudaFree(insts_);
         cudaFree(ranges_);
         cudaFree(counter_);
@@ -290,6 +368,8 @@ template <class T> class Batch2 final : public BatchBase {
         if (own_stream_) cudaStreamDestroy(stream_);
     }
 
+    // 2D rows are padded to a 16-byte multiple (one spare cell for odd NB_Y in FP32) so
+    // that every instance can be fed by TMA; 3D keeps the reference strides.
     static size_t row_stride(size_t nb_y)
     {
         const size_t per = 16 / (2 * sizeof(T)); // cells per 16 bytes of one pair array
@@ -298,19 +378,20 @@ template <class T> class Batch2 final : public BatchBase {
 
     size_t bytes(const hydro_blast_t &s) const override
     {
-        return 2 * 4 * sizeof(T) * (s.nb[0] + 2) * row_stride(s.nb[1]);
+        if constexpr (D == 2) return 2 * 4 * sizeof(T) * (s.nb[0] + 2) * row_stride(s.nb[1]);
+        else return 2 * 5 * sizeof(T) * (s.nb[0] + 2) * (s.nb[1] + 2) * (s.nb[2] + 2);
     }
 
     int add(const hydro_blast_t &s) override
     {
-        const size_t nb_x = s.nb[0], nb_y = s.nb[1];
-        if (nb_x == 0 || nb_y == 0 || nb_x > (1u << 24) || nb_y > (1u << 24) || !(s.gamma > 1.0)) {
-            set_error(kErrArg, "batch add: invalid blast (grid %zu x %zu, gamma %g)", nb_x, nb_y, s.gamma);
+        const size_t nb_x = s.nb[0], nb_y = s.nb[1], nb_z = (D == 3) ? s.nb[2] : 0;
+        const size_t lim = D == 2 ? (1u << 24) : (1u << 14);
+        if (nb_x == 0 || nb_y == 0 || nb_x > lim || nb_y > lim || (D == 3 && (nb_z == 0 || nb_z > lim)) ||
+            !(s.gamma > 1.0)) {
+            set_error(kErrArg, "batch add: invalid %dD blast (grid %zu x %zu x %zu, gamma %g)", D, nb_x, nb_y, nb_z,
+                      s.gamma);
             return kErrArg;
         }
-        // the batch owns its layout: rows are padded to a 16-byte multiple (one spare
-        // cell for odd NB_Y in FP32) so that every instance can be fed by TMA
-        const size_t ys = row_stride(nb_y), rowbytes = 2 * sizeof(T) * ys;
         int slot = -1;
         for (int i = 0; i < cap_; ++i)
             if (!slots_[i].used) {
@@ -322,29 +403,31 @@ template <class T> class Batch2 final : public BatchBase {
             return kErrArg;
         }
         Slot &sl = slots_[slot];
-        const size_t n = 2 * ys * (nb_x + 2);
+        const size_t ys = (D == 2) ? row_stride(nb_y) : nb_y + 2;
+        const size_t ncell = (D == 2) ? ys * (nb_x + 2) : (nb_x + 2) * (nb_y + 2) * (nb_z + 2);
+        const size_t nv = (D == 2) ? 2 : 3;
         cudaError_t e = cudaSuccess;
         for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-            e = cudaMallocAsync(&sl.rhoE[b], n * sizeof(T), stream_);
-            if (e == cudaSuccess) e = cudaMallocAsync(&sl.uv[b], n * sizeof(T), stream_);
-            if (e == cudaSuccess) e = cudaMemsetAsync(sl.rhoE[b], 0, n * sizeof(T), stream_);
-            if (e == cudaSuccess) e = cudaMemsetAsync(sl.uv[b], 0, n * sizeof(T), stream_);
+            e = cudaMallocAsync(&sl.rhoE[b], 2 * ncell * sizeof(T), stream_);
+            if (e == cudaSuccess) e = cudaMallocAsync(&sl.uvx[b], nv * ncell * sizeof(T), stream_);
+            if (e == cudaSuccess) e = cudaMemsetAsync(sl.rhoE[b], 0, 2 * ncell * sizeof(T), stream_);
+            if (e == cudaSuccess) e = cudaMemsetAsync(sl.uvx[b], 0, nv * ncell * sizeof(T), stream_);
         }
         if (e != cudaSuccess) {
             set_error(kErrCuda, "batch add: allocation of %zu bytes failed: %s", bytes(s), cudaGetErrorString(e));
-            for (int b = 0; b < 2; ++b) {
-                if (sl.rhoE[b]) cudaFreeAsync(sl.rhoE[b], stream_);
-                if (sl.uv[b]) cudaFreeAsync(sl.uv[b], stream_);
-                sl.rhoE[b] = sl.uv[b] = nullptr;
-            }
+            free_slot(sl);
             return kErrCuda;
         }
-        Inst2<T> I;
+        Inst I;
         memset(&I, 0, sizeof I);
         const T one = T(1);
         I.DX = one / T(nb_x + 1);
         I.DY = one / T(nb_y + 1);
-        const T ms = (I.DY < I.DX) ? I.DY : I.DX;
+        T ms = (I.DY < I.DX) ? I.DY : I.DX; // std::min({DX, DY[, DZ]}) (main.cxx:484)
+        if constexpr (D == 3) {
+            I.DZ = one / T(nb_z + 1);
+            ms = (I.DZ < ms) ? I.DZ : ms;
+        }
         I.ph.C_min = T(T(s.C) * ms);
         I.ph.gamma = T(s.gamma);
         I.ph.gm1 = T(I.ph.gamma - one);
@@ -352,9 +435,15 @@ template <class T> class Batch2 final : public BatchBase {
         I.ph.K = T(s.K);
         I.ph.kneg = I.ph.K < T(0);
         T first = 0;
-        int rc = init2d_at<T>(sl.rhoE[0], sl.uv[0], nb_x, nb_y, s.centre[0], s.centre[1], s.radius, T(s.rho_in),
+        int rc;
+        if constexpr (D == 2)
+            rc = init2d_at<T>(sl.rhoE[0], sl.uvx[0], nb_x, nb_y, s.centre[0], s.centre[1], s.radius, T(s.rho_in),
                               T(s.rho_out), T(s.p_in), T(s.p_out), I.ph.C_min, I.ph.gamma, &first, stream_,
                               scratch_bits_, (long long)ys);
+        else
+            rc = init3d_at<T>(sl.rhoE[0], sl.uvx[0], nb_x, nb_y, nb_z, s.centre[0], s.centre[1], s.centre[2],
+                              s.radius, T(s.rho_in), T(s.rho_out), T(s.p_in), T(s.p_out), I.ph.C_min, I.ph.gamma,
+                              &first, stream_, scratch_bits_);
         if (rc != kOk) {
             free_slot(sl);
             return rc;
@@ -369,21 +458,39 @@ template <class T> class Batch2 final : public BatchBase {
         I.steps = 0;
         I.nb_x = (int)nb_x;
         I.nb_y = (int)nb_y;
-        I.ys = (long long)ys;
-        I.nstrips = (int)((nb_y + kStripW - 1) / kStripW);
         I.chunk = chunk_;
         I.parity = 0;
         I.active = (0.0 < s.t_end) && (0 < s.max_steps);
-        for (int b = 0; b < 2; ++b) {
-            I.rhoE[b] = sl.rhoE[b];
-            I.uv[b] = sl.uv[b];
-            const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-            if (!encode_tmap_2d(&I.tm[b][0], dt, sl.rhoE[b], 2 * ys, nb_x + 2, rowbytes, 2 * kStripNT, 1) ||
-                !encode_tmap_2d(&I.tm[b][1], dt, sl.uv[b], 2 * ys, nb_x + 2, rowbytes, 2 * kStripNT, 1)) {
-                free_slot(sl);
-                set_error(kErrCuda, "batch add: tensor map encoding failed");
-                return kErrCuda;
+        int nitems;
+        if constexpr (D == 2) {
+            I.ys = (long long)ys;
+            I.nstrips = (int)((nb_y + kStripW - 1) / kStripW);
+            const size_t rowbytes = 2 * sizeof(T) * ys;
+            const CUtensorMapDataType dt =
+                sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+            for (int b = 0; b < 2; ++b) {
+                I.rhoE[b] = sl.rhoE[b];
+                I.uv[b] = sl.uvx[b];
+                if (!encode_tmap_2d(&I.tm[b][0], dt, sl.rhoE[b], 2 * (nb_y + 2), nb_x + 2, rowbytes, 2 * kStripNT, 1) ||
+                    !encode_tmap_2d(&I.tm[b][1], dt, sl.uvx[b], 2 * (nb_y + 2), nb_x + 2, rowbytes, 2 * kStripNT, 1)) {
+                    free_slot(sl);
+                    set_error(kErrCuda, "batch add: tensor map encoding failed");
+                    return kErrCuda;
+                }
             }
+            nitems = I.nstrips * (int)((nb_x + chunk_ - 1) / chunk_);
+        } else {
+            I.DtDz = I.dt / I.DZ;
+            I.nb_z = (int)nb_z;
+            I.zs = (long long)nb_z + 2;
+            I.zy = (long long)(nb_y + 2) * I.zs;
+            I.ntz = (int)((nb_z + k3TZ - 1) / k3TZ);
+            I.nty = (int)((nb_y + k3TY - 1) / k3TY);
+            for (int b = 0; b < 2; ++b) {
+                I.rhoE[b] = sl.rhoE[b];
+                I.uvw[b] = sl.uvx[b];
+            }
+            nitems = I.ntz * I.nty * (int)((nb_x + chunk_ - 1) / chunk_);
         }
         e = cudaMemcpyAsync(insts_ + slot, &I, sizeof I, cudaMemcpyHostToDevice, stream_);
         SlotStatus st0{};
@@ -397,11 +504,11 @@ template <class T> class Batch2 final : public BatchBase {
             return kErrCuda;
         }
         sl.used = true;
-        sl.nitems = I.nstrips * (int)((nb_x + chunk_ - 1) / chunk_);
-        sl.bytes = bytes(s);
+        sl.nitems = nitems;
         sl.ys = ys;
-        sl.nb_x = nb_x;
-        sl.nb_y = nb_y;
+        sl.nb[0] = nb_x;
+        sl.nb[1] = nb_y;
+        sl.nb[2] = nb_z;
         dirty_ = true;
         return slot;
     }
@@ -471,7 +578,7 @@ template <class T> class Batch2 final : public BatchBase {
         // the current buffer is the one the last completed step wrote: parity of steps
         const int par = (int)(status_h_[slot].steps & 1);
         *rhoE = slots_[slot].rhoE[par];
-        *uvx = slots_[slot].uv[par];
+        *uvx = slots_[slot].uvx[par];
         if (row_stride) *row_stride = (long long)slots_[slot].ys;
         return kOk;
     }
@@ -483,10 +590,17 @@ template <class T> class Batch2 final : public BatchBase {
         int rc = state(slot, &r, &u, &ys);
         if (rc != kOk) return rc;
         const Slot &sl = slots_[slot];
-        const size_t w = 2 * sizeof(T) * (sl.nb_y + 2), sp = 2 * sizeof(T) * (size_t)ys;
         const cudaMemcpyKind k = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-        cudaError_t e = cudaMemcpy2DAsync(rhoE, w, r, sp, w, sl.nb_x + 2, k, stream_);
-        if (e == cudaSuccess) e = cudaMemcpy2DAsync(uvx, w, u, sp, w, sl.nb_x + 2, k, stream_);
+        cudaError_t e;
+        if constexpr (D == 2) {
+            const size_t w = 2 * sizeof(T) * (sl.nb[1] + 2), sp = 2 * sizeof(T) * (size_t)ys;
+            e = cudaMemcpy2DAsync(rhoE, w, r, sp, w, sl.nb[0] + 2, k, stream_);
+            if (e == cudaSuccess) e = cudaMemcpy2DAsync(uvx, w, u, sp, w, sl.nb[0] + 2, k, stream_);
+        } else {
+            const size_t n = (sl.nb[0] + 2) * (sl.nb[1] + 2) * (sl.nb[2] + 2) * sizeof(T);
+            e = cudaMemcpyAsync(rhoE, r, 2 * n, k, stream_);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(uvx, u, 3 * n, k, stream_);
+        }
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
         if (e != cudaSuccess) {
             set_error(kErrCuda, "batch copy_state: %s", cudaGetErrorString(e));
@@ -495,24 +609,43 @@ template <class T> class Batch2 final : public BatchBase {
         return kOk;
     }
 
+    int sync() override
+    {
+        const cudaError_t e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) {
+            set_error(kErrCuda, "batch sync: %s", cudaGetErrorString(e));
+            return kErrCuda;
+        }
+        return kOk;
+    }
+
   private:
     struct Slot {
         bool used = false;
-        T *rhoE[2] = {nullptr, nullptr}, *uv[2] = {nullptr, nullptr};
+        T *rhoE[2] = {nullptr, nullptr}, *uvx[2] = {nullptr, nullptr};
         int nitems = 0;
-        size_t bytes = 0;
-        size_t ys = 0, nb_x = 0, nb_y = 0;
+        size_t ys = 0, nb[3] = {0, 0, 0};
     };
 
     void free_slot(Slot &s)
     {
         for (int b = 0; b < 2; ++b) {
             if (s.rhoE[b]) cudaFreeAsync(s.rhoE[b], stream_);
-            if (s.uv[b]) cudaFreeAsync(s.uv[b], stream_);
-            s.rhoE[b] = s.uv[b] = nullptr;
+            if (s.uvx[b]) cudaFreeAsync(s.uvx[b], stream_);
+            s.rhoE[b] = s.uvx[b] = nullptr;
         }
         s.used = false;
         s.nitems = 0;
+    }
+
+    void launch()
+    {
+        if constexpr (D == 2)
+            batch2d<T><<<blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
+                                                         status_d_);
+        else
+            batch3d<T><<<blocks_, k3NT, smem_, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
+                                                         status_d_);
     }
 
     // Work list and partial slots for the instances in use; the graph of `nsteps` steps.
@@ -554,8 +687,7 @@ template <class T> class Batch2 final : public BatchBase {
             for (int k = 0; k < nsteps && e == cudaSuccess; ++k) {
                 e = cudaMemsetAsync(counter_, 0, sizeof(unsigned), stream_);
                 if (e == cudaSuccess) {
-                    batch2d<T><<<blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
-                                                                 status_d_);
+                    launch();
                     e = cudaGetLastError();
                 }
             }
@@ -576,7 +708,7 @@ template <class T> class Batch2 final : public BatchBase {
     int chunk_, cap_;
     bool own_stream_ = false, dirty_ = true;
     cudaStream_t stream_ = nullptr;
-    Inst2<T> *insts_ = nullptr;
+    Inst *insts_ = nullptr;
     int2 *ranges_ = nullptr, *items_ = nullptr;
     size_t items_cap_ = 0;
     ItemPart *parts_ = nullptr;
@@ -585,7 +717,7 @@ template <class T> class Batch2 final : public BatchBase {
     SlotStatus *status_h_ = nullptr, *status_d_ = nullptr;
     std::vector<Slot> slots_;
     std::vector<int2> host_ranges_;
-    int nitems_ = 0, blocks_ = 148, graph_steps_ = -1;
+    int nitems_ = 0, blocks_ = 148, graph_steps_ = -1, smem_ = 0;
     cudaGraphExec_t graph_ = nullptr;
 };
 
@@ -597,16 +729,19 @@ extern "C" {
 
 void *hydro_batch_create(int dim, int precision_bytes, int chunk, int capacity, void *stream)
 {
-    if (dim != 2 || (precision_bytes != 4 && precision_bytes != 8) || capacity <= 0 || capacity > (1 << 20) ||
-        chunk < 0) {
+    if ((dim != 2 && dim != 3) || (precision_bytes != 4 && precision_bytes != 8) || capacity <= 0 ||
+        capacity > (1 << 20) || chunk < 0) {
         set_error(kErrArg, "hydro_batch_create: unsupported (dim %d, precision %d bytes, capacity %d)", dim,
                   precision_bytes, capacity);
         return nullptr;
     }
     int rc = kOk;
     BatchBase *b = nullptr;
-    if (precision_bytes == 8) b = new Batch2<double>(chunk, capacity, (cudaStream_t)stream, &rc);
-    else b = new Batch2<float>(chunk, capacity, (cudaStream_t)stream, &rc);
+    const cudaStream_t s = (cudaStream_t)stream;
+    if (dim == 2 && precision_bytes == 8) b = new BatchEngine<double, 2>(chunk, capacity, s, &rc);
+    else if (dim == 2) b = new BatchEngine<float, 2>(chunk, capacity, s, &rc);
+    else if (precision_bytes == 8) b = new BatchEngine<double, 3>(chunk, capacity, s, &rc);
+    else b = new BatchEngine<float, 3>(chunk, capacity, s, &rc);
     if (rc != kOk) {
         delete b;
         return nullptr;
@@ -647,18 +782,65 @@ int hydro_batch_state(void *b, int slot, const void **rhoE, const void **uvx, lo
     return static_cast<BatchBase *>(b)->state(slot, rhoE, uvx, row_stride);
 }
 
-long long hydro_batch_bytes(void *b, const hydro_blast_t *spec)
-{
-    if (!b || !spec) return kErrArg;
-    return (long long)static_cast<BatchBase *>(b)->bytes(*spec);
-}
-
 int hydro_batch_copy_state(void *b, int slot, void *rhoE, void *uvx, int to_host)
 {
     if (!b || !rhoE || !uvx) return kErrArg;
     return static_cast<BatchBase *>(b)->copy_state(slot, rhoE, uvx, to_host != 0);
 }
 
+long long hydro_batch_bytes(void *b, const hydro_blast_t *spec)
+{
+    if (!b || !spec) return kErrArg;
+    return (long long)static_cast<BatchBase *>(b)->bytes(*spec);
+}
+
+int hydro_batch_sync(void *b)
+{
+    if (!b) return kErrArg;
+    return static_cast<BatchBase *>(b)->sync();
+}
+
 void hydro_batch_destroy(void *b) { delete static_cast<BatchBase *>(b); }
+
+int hydro2d_init_blast_at_f64(double *d_rhoE, double *d_uv, size_t NB_X, size_t NB_Y, double cx, double cy,
+                              double radius, double rho_in, double rho_out, double p_in, double p_out, double C_min,
+                              double gamma, double *min_dt, void *stream)
+{
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    return init2d_at<double>(d_rhoE, d_uv, NB_X, NB_Y, cx, cy, radius, rho_in, rho_out, p_in, p_out, C_min, gamma,
+                             min_dt, (cudaStream_t)stream, &ctx->scr->max_bits);
+}
+int hydro2d_init_blast_at_f32(float *d_rhoE, float *d_uv, size_t NB_X, size_t NB_Y, double cx, double cy,
+                              double radius, float rho_in, float rho_out, float p_in, float p_out, float C_min,
+                              float gamma, float *min_dt, void *stream)
+{
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    return init2d_at<float>(d_rhoE, d_uv, NB_X, NB_Y, cx, cy, radius, rho_in, rho_out, p_in, p_out, C_min, gamma,
+                            min_dt, (cudaStream_t)stream, &ctx->scr->max_bits);
+}
+int hydro3d_init_blast_at_f64(double *d_rhoE, double *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, double cx,
+                              double cy, double cz, double radius, double rho_in, double rho_out, double p_in,
+                              double p_out, double C_min, double gamma, double *min_dt, void *stream)
+{
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    return init3d_at<double>(d_rhoE, d_uvw, NB_X, NB_Y, NB_Z, cx, cy, cz, radius, rho_in, rho_out, p_in, p_out,
+                             C_min, gamma, min_dt, (cudaStream_t)stream, &ctx->scr->max_bits);
+}
+int hydro3d_init_blast_at_f32(float *d_rhoE, float *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, double cx,
+                              double cy, double cz, double radius, float rho_in, float rho_out, float p_in,
+                              float p_out, float C_min, float gamma, float *min_dt, void *stream)
+{
+    int err;
+    DevCtx *ctx = ctx_current(&err);
+    if (!ctx) return err;
+    return init3d_at<float>(d_rhoE, d_uvw, NB_X, NB_Y, NB_Z, cx, cy, cz, radius, rho_in, rho_out, p_in, p_out,
+                            C_min, gamma, min_dt, (cudaStream_t)stream, &ctx->scr->max_bits);
+}
 
 } // extern "C"

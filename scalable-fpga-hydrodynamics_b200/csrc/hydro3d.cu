@@ -21,6 +21,7 @@
 #include <stdio.h>
 
 #include "hydro_host.h"
+#include "strip3d_march.cuh"
 
 namespace hydro {
 
@@ -41,7 +42,6 @@ template <class T> struct Args3 {
     float ggm1;             // gamma * (gamma - 1), for the speed upper bound
 };
 
-__device__ __forceinline__ int wrap_plane(int n, int nb_x) { return n == 0 ? nb_x : (n == nb_x + 1 ? 1 : n); }
 
 template <class T> __device__ __forceinline__ Cell3<T> load_cell3(const Args3<T> &g, long long c)
 {
@@ -105,162 +105,23 @@ template <class T> __global__ void __launch_bounds__(k3RedoNT) redo3d(Args3<T> g
 }
 
 // ------------------------------------------------------------------- strip kernel ---
-constexpr int k3Warps = 8;                 // y extent of the tile (with halo)
-constexpr int k3NT = 32 * k3Warps;         // threads
-constexpr int k3TY = k3Warps - 2;          // interior rows per tile
-constexpr int k3TZ = 30;                   // interior columns per tile
-constexpr int k3Stages = 4;
-
-__device__ __forceinline__ void cp_async(void *dst, const void *src, int bytes, bool valid)
-{
-    const uint32_t d = smem_u32(dst);
-    const int n = valid ? bytes : 0;
-    if (bytes == 16)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-    else if (bytes == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-template <class T> struct Smem3 {
-    T st[k3Stages][5][k3NT];      // per plane: rho, E, rho_u, rho_v, rho_w
-    T xP[2][9][k3NT];             // y-face inputs of each lane's cell, by plane parity
-    T xF[2][5][k3NT];             // each lane's +y face flux, by plane parity
-};
-
 template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem3<T> &S = *reinterpret_cast<Smem3<T> *>(smem_raw);
-    constexpr unsigned FULL = 0xffffffffu;
-
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    const int kbase = k3TZ * blockIdx.x, jbase = k3TY * blockIdx.y;
-    const int k = kbase + lane, j = jbase + w;
-    const int i0 = 1 + g.chunk * blockIdx.z;
-    const int i1 = min(i0 + g.chunk - 1, g.nb_x);
-    const int nplanes = i1 - i0 + 3;
-    const bool in_array = (j <= g.nb_y + 1) && (k <= g.nb_z + 1);
-    const bool interior = (w >= 1) && (w <= k3TY) && (lane >= 1) && (lane <= k3TZ) && (j <= g.nb_y) && (k <= g.nb_z);
-    const bool iwarp = (w >= 1) && (w <= k3TY) && (jbase + 1 <= g.nb_y); // warp holds interior rows
-    const long long colofs = (long long)j * g.zs + k;
-
-    auto issue = [&](int m) {
-        const int s = m % k3Stages;
-        if (m < nplanes) {
-            const long long c = (long long)wrap_plane(i0 - 1 + m, g.nb_x) * g.zy + colofs;
-            const T *pr = in_array ? g.rhoE + 2 * c : g.rhoE;
-            const T *pu = in_array ? g.uvw + 3 * c : g.uvw;
-            cp_async(&S.st[s][0][t], pr, sizeof(T), in_array);
-            cp_async(&S.st[s][1][t], pr + 1, sizeof(T), in_array);
-            cp_async(&S.st[s][2][t], pu, sizeof(T), in_array);
-            cp_async(&S.st[s][3][t], pu + 1, sizeof(T), in_array);
-            cp_async(&S.st[s][4][t], pu + 2, sizeof(T), in_array);
-        }
-        cp_async_commit();
-    };
-#pragma unroll
-    for (int m = 0; m < k3Stages - 1; ++m) issue(m);
-
+    const int i0 = 1 + g.chunk * (int)blockIdx.z;
+    const March3 geo{k3TZ * (int)blockIdx.x, k3TY * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
+                     g.nb_x, g.nb_y, g.nb_z, g.zs, g.zy};
     StepAcc acc;
-    Cell3<T> Pm{};
-    T Ur = 0, Uu = 0, Uv = 0, Uw = 0, UE = 0;
-    Flux3<T> fxlo{};
     const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
-    // ghost cells (j or k = 0 or NB+1) and cells past the array are never used: they
-    // convert a unit state so every lane's reciprocal / square root stays regular
-    const bool real = (j >= 1) && (j <= g.nb_y) && (k >= 1) && (k <= g.nb_z);
-#pragma unroll 2
-    for (int m = 0; m < nplanes; ++m) {
-        issue(m + k3Stages - 1);
-        cp_async_wait<k3Stages - 1>();
-        const int s = m % k3Stages;
-        const T ur = real ? S.st[s][0][t] : T(1), uE = real ? S.st[s][1][t] : T(1);
-        const T uu = real ? S.st[s][2][t] : T(0), uv = real ? S.st[s][3][t] : T(0);
-        const T uw = real ? S.st[s][4][t] : T(0);
-        const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, g.ph);
-        {
-            const FaceIn3<T> fy = face3_y(P);
-            T *x = &S.xP[m & 1][0][t];
-            x[0 * k3NT] = fy.r; x[1 * k3NT] = fy.un; x[2 * k3NT] = fy.p; x[3 * k3NT] = fy.Ka;
-            x[4 * k3NT] = fy.iKa; x[5 * k3NT] = fy.mn; x[6 * k3NT] = fy.mt1; x[7 * k3NT] = fy.mt2;
-            x[8 * k3NT] = fy.eup;
-        }
-        Flux3<T> fxhi{};
-        if (m >= 1 && iwarp) fxhi = face_flux3(face3_x(Pm), face3_x(P), g.ph);
-
-        // faces of plane m-1 (an interior plane when 2 <= m)
-        if (m >= 2) {
-            // +y face of (j | j+1), from this lane's previous-plane cell and the warp above's
-            const FaceIn3<T> me = face3_y(Pm);
-            Flux3<T> fy{};
-            if (w < k3Warps - 1) {
-                const T *x = &S.xP[(m - 1) & 1][0][t + 32];
-                FaceIn3<T> nb{x[0 * k3NT], x[1 * k3NT], x[2 * k3NT], x[3 * k3NT], x[4 * k3NT],
-                              x[5 * k3NT], x[6 * k3NT], x[7 * k3NT], x[8 * k3NT]};
-                FaceIn3<T> L = me, R = nb;
-                if (j == 0) L = mirror3(nb);
-                if (j == g.nb_y) R = mirror3(me);
-                fy = face_flux3(L, R, g.ph);
-                T *xf = &S.xF[m & 1][0][t];
-                xf[0 * k3NT] = fy.r; xf[1 * k3NT] = fy.n; xf[2 * k3NT] = fy.t1; xf[3 * k3NT] = fy.t2;
-                xf[4 * k3NT] = fy.E;
-            }
-            // +z face of (k | k+1) via shuffles within the warp
-            Flux3<T> fz{};
-            if (iwarp) {
-                const FaceIn3<T> mz = face3_z(Pm);
-                FaceIn3<T> nz;
-                nz.r = __shfl_down_sync(FULL, mz.r, 1);
-                nz.un = __shfl_down_sync(FULL, mz.un, 1);
-                nz.p = __shfl_down_sync(FULL, mz.p, 1);
-                nz.Ka = __shfl_down_sync(FULL, mz.Ka, 1);
-                nz.iKa = __shfl_down_sync(FULL, mz.iKa, 1);
-                nz.mn = __shfl_down_sync(FULL, mz.mn, 1);
-                nz.mt1 = __shfl_down_sync(FULL, mz.mt1, 1);
-                nz.mt2 = __shfl_down_sync(FULL, mz.mt2, 1);
-                nz.eup = __shfl_down_sync(FULL, mz.eup, 1);
-                FaceIn3<T> L = mz, R = nz;
-                if (k == 0) L = mirror3(nz);
-                if (k == g.nb_z) R = mirror3(mz);
-                fz = face_flux3(L, R, g.ph);
-            }
-            __syncthreads(); // +y faces of this plane published
-            if (iwarp) {
-                Flux3<T> fzl;
-                fzl.r = __shfl_up_sync(FULL, fz.r, 1);
-                fzl.n = __shfl_up_sync(FULL, fz.n, 1);
-                fzl.t1 = __shfl_up_sync(FULL, fz.t1, 1);
-                fzl.t2 = __shfl_up_sync(FULL, fz.t2, 1);
-                fzl.E = __shfl_up_sync(FULL, fz.E, 1);
-                if (interior) {
-                    const T *xf = &S.xF[m & 1][0][t - 32];
-                    const Flux3<T> fyl{xf[0 * k3NT], xf[1 * k3NT], xf[2 * k3NT], xf[3 * k3NT], xf[4 * k3NT]};
-                    const Upd3<T> o = update3(Ur, Uu, Uv, Uw, UE, fxlo, fxhi, fyl, fy, fzl, fz, g.DtDx, g.DtDy,
-                                              g.DtDz, g.ph);
-                    const long long c = (long long)(i0 + m - 2) * g.zy + colofs;
-                    g.rhoE_n[2 * c] = o.r;
-                    g.rhoE_n[2 * c + 1] = o.E;
-                    g.uvw_n[3 * c] = o.u;
-                    g.uvw_n[3 * c + 1] = o.v;
-                    g.uvw_n[3 * c + 2] = o.w;
-                    acc.add_mass(o.r);
-                    const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
-                    const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, g.ggm1);
-                    if (!(ub < tlof)) acc.add_speed(speed3(o.r, o.u, o.v, o.w, o.E, g.ph));
-                }
-            }
-        } else {
-            __syncthreads(); // keep one barrier per plane: publishes this plane's xP
-        }
-        fxlo = fxhi;
-        Pm = P;
-        Ur = ur; Uu = uu; Uv = uv; Uw = uw; UE = uE;
-    }
-    cp_async_wait<0>();
+    const float ggm1 = g.ggm1;
+    const Phys<T> ph = g.ph;
+    march3d<T>(S, g.rhoE, g.uvw, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz, [&](const Upd3<T> &o) {
+        acc.add_mass(o.r);
+        const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
+        const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1);
+        if (!(ub < tlof)) acc.add_speed(speed3(o.r, o.u, o.v, o.w, o.E, ph));
+    });
     step_epilogue<k3NT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
                            blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
                            g.status, g.seq, (double)tlof, g.key);
