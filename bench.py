@@ -34,7 +34,6 @@ import sys
 import tempfile
 import threading
 import time
-from datetime import timedelta
 from pathlib import Path
 
 import numpy as np
@@ -139,7 +138,9 @@ def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0):
     total_ms = e_start.elapsed_time(e_end)
     kern_ms = [a.elapsed_time(b) for a, b in per]
     info = run.last_info
-    res = dict(total_ms=total_ms, kernel_ms=kern_ms, kernel=int(info.kernel), it=run.it)
+    # an asynchronous step launches the update kernel and the signal-speed check kernel
+    # (which returns at once unless the fused maximum fell under its skip threshold)
+    res = dict(total_ms=total_ms, kernel_ms=kern_ms, kernel=int(info.kernel), it=run.it, launches_per_step=2)
     del run
     torch.cuda.empty_cache()
     return res
@@ -281,6 +282,118 @@ def cpu_reference_sample(nb_y: int, rows: int, seconds: float, threads: int):
     return cells / (t1 - t0), kind, what
 
 
+# --------------------------------------------------------------- batched / serving ---
+def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, log=print):
+    """The batched workload (256 seeded 2D blasts, sides log-uniform in [64, 2048], 200
+    steps each) through the FP32 and FP64 batch engines (chunk from the autotuner), and the
+    same instances one at a time through the plain FP64 path. Accuracy: FP32 against the
+    FP64 batch (bit-identical to the plain FP64 path) on every instance."""
+    from hydro_b200.autotune import tune
+    from hydro_b200.batch import Batch
+    from hydro_b200.workloads import batch_blasts
+
+    out = {}
+    blasts = batch_blasts(n, seed=seed, steps=steps)
+    cells = sum(int(np.prod(b.nb)) for b in blasts)
+    states = {}
+    for T in (np.float32, np.float64):
+        chunk = tune(2, T, log=log)
+        s = torch.cuda.Stream()
+        # warm-up: a throw-away batch of the same instances runs a few steps
+        w = Batch(2, T, chunk=chunk, capacity=n, stream=s)
+        for bl in blasts[:32]:
+            w.add(bl)
+        w.run(3)
+        w.close()
+        b = Batch(2, T, chunk=chunk, capacity=n, stream=s)
+        slots = [b.add(bl) for bl in blasts]
+        b.prepare(steps)  # graph captured and instantiated outside the timed region
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(s)
+        b.run(steps, sync=False)
+        e1.record(s)
+        b.sync()
+        wall = time.perf_counter() - t0
+        ms = e0.elapsed_time(e1)
+        done = sum(b.status(k)["steps"] for k in slots)
+        assert done == n * steps, (done, n * steps)
+        key = "fp32" if T is np.float32 else "fp64"
+        out[f"batched_{key}"] = dict(value=cells * steps / (ms / 1e3) / 1e9, unit=UNIT, ms=ms, wall_s=wall,
+                                     chunk=chunk, instances=n, steps=steps, cells=cells,
+                                     bytes_per_cell=32 if T is np.float32 else 64)
+        states[key] = [b.state(k)[0] for k in slots]
+        b.close()
+    # accuracy of the FP32 batch against FP64 (rho, relative L1 and L-inf per instance)
+    l1, linf = [], []
+    for a, r, bl in zip(states["fp32"], states["fp64"], blasts):
+        sh = tuple(x + 2 for x in bl.nb) + (2,)
+        inner = tuple(slice(1, x + 1) for x in bl.nb)
+        ra = a.reshape(sh)[inner][..., 0].astype(np.float64)
+        rr = r.reshape(sh)[inner][..., 0]
+        l1.append(np.abs(ra - rr).sum() / np.abs(rr).sum())
+        linf.append(np.abs(ra - rr).max() / np.abs(rr).max())
+    out["batched_fp32"]["rho_rel_l1_vs_fp64_max"] = float(max(l1))
+    out["batched_fp32"]["rho_rel_linf_vs_fp64_max"] = float(max(linf))
+    # plain FP64 path, one instance at a time (the reference host loop per instance)
+    sample = blasts if plain_sample is None else blasts[:plain_sample]
+    pcells = sum(int(np.prod(b.nb)) for b in sample)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for bl in sample:
+        hb.BlastRun(bl.nb, np.float64, blast=bl).run(float("inf"), steps)
+    torch.cuda.synchronize()
+    pw = time.perf_counter() - t0
+    out["plain_fp64_one_at_a_time"] = dict(value=pcells * steps / pw / 1e9, unit=UNIT, wall_s=pw,
+                                           instances=len(sample), steps=steps)
+    out["batched_fp32_over_plain_fp64"] = out["batched_fp32"]["value"] / out["plain_fp64_one_at_a_time"]["value"]
+    return out
+
+
+def bench_serving(hb, torch, rates=(10.0, 1000.0), nreq=8, seed=0, max_wall=20.0, plain=True, log=print):
+    """The serving workload: Poisson streams of mixed requests (70% 2D sides [128, 4096],
+    30% 3D sides [32, 256], t_end in [0.05, 0.5] of the sound-crossing time, FP32/FP64 50/50),
+    `nreq` requests per rate, through the continuous-batching server (150 GB budget) and
+    through the plain path one request at a time, each request in its own precision. At the
+    highest rate the same stream also runs all-FP32 through the server against all-FP64
+    through the plain path. Each run is capped at `max_wall` seconds: latency percentiles
+    cover the completed requests, throughput all the cell-updates done within the run."""
+    from hydro_b200.autotune import best_chunk
+    from hydro_b200.serving import Server, serve_plain, summarize
+    from hydro_b200.workloads import request_stream
+
+    def served(reqs, dtype=None):
+        srv = Server(hbm_budget=150e9, steps_per_tick=8, chunk2d=best_chunk(2, np.float32),
+                     chunk3d=best_chunk(3, np.float32))
+        recs, wall = srv.serve(reqs, max_wall=max_wall, dtype=dtype)
+        srv.close()
+        torch.cuda.empty_cache()
+        return summarize(recs, wall)
+
+    def plain_path(reqs, dtype=None):
+        recs, wall = serve_plain(reqs, max_wall=max_wall, dtype=dtype)
+        torch.cuda.empty_cache()
+        return summarize(recs, wall)
+
+    res = {}
+    for rate in rates:
+        reqs = request_stream(rate, seed=seed, count=nreq)
+        entry = dict(batched=served(reqs))
+        if plain:
+            entry["plain_one_at_a_time"] = plain_path(reqs)
+            entry["batched_over_plain"] = entry["batched"]["gcell_s"] / max(entry["plain_one_at_a_time"]["gcell_s"],
+                                                                            1e-30)
+        if plain and rate == max(rates):
+            entry["batched_fp32"] = served(reqs, np.float32)
+            entry["plain_fp64"] = plain_path(reqs, np.float64)
+            entry["batched_fp32_over_plain_fp64"] = entry["batched_fp32"]["gcell_s"] / max(
+                entry["plain_fp64"]["gcell_s"], 1e-30)
+        res[f"rate_{rate:g}"] = entry
+        log(f"serving rate {rate:g}/s: {json.dumps(entry)}")
+    return res
+
+
 # ------------------------------------------------------------------------ main ---
 def main():
     ap = argparse.ArgumentParser()
@@ -295,6 +408,12 @@ def main():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-rates", type=float, nargs="+", default=[10.0, 1000.0])
+    ap.add_argument("--serving-requests", type=int, default=8)
+    ap.add_argument("--serving-wall", type=float, default=20.0, help="cap per serving run, seconds")
+    ap.add_argument("--no-serving-plain", action="store_true")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.nb != [40000, 20000], "at least 3 warm-up steps"
 
@@ -334,23 +453,10 @@ def main():
     hb = load_pkg()
     hb.build()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
+    from hydro_b200.replicas import Replicas
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+    reps = Replicas("nccl", timeout_s=300)
+    max_over_ranks, barrier = reps.max_over_ranks, reps.barrier
 
     hbm, peak_kind = peaks()
     cells = int(np.prod(nb))
@@ -403,6 +509,17 @@ def main():
                                   kernel_gbs=vc * bpc / (km / 1e3) / 1e9, frac=vc * bpc / (km / 1e3) / 1e9 / hbm,
                                   kernel=int(vr["kernel"]), ms_per_step=vms / nst)
 
+    log = lambda msg: print(msg, file=sys.stderr, flush=True)
+    batched = serving = None
+    if rank == 0 and world == 1 and not args.no_batched and args.case == "2d_f64":
+        barrier()
+        batched = bench_batched(hb, torch, log=log)
+        torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_serving and args.case == "2d_f64":
+        serving = bench_serving(hb, torch, rates=tuple(args.serving_rates), nreq=args.serving_requests,
+                                max_wall=args.serving_wall, plain=not args.no_serving_plain, log=log)
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and dim == 2:
         thr = cpu_threads()
@@ -417,12 +534,11 @@ def main():
                     config=dict(workload=workload, nb=list(nb),
                                 l2=f"inputs larger than L2 ({cells * bpc / 2 / 1e9:.1f} GB state, 126 MB L2)",
                                 parallelism=f"replicas x{world}"),
-                    roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps, clocks=clocks,
-                    variants=variants)
+                    roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps * r["launches_per_step"],
+                    clocks=clocks, variants=variants, batched=batched, serving=serving)
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.barrier()
+    reps.close()
 
 
 if __name__ == "__main__":

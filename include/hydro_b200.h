@@ -215,6 +215,9 @@ int hydro_batch_state(void *batch, int slot, const void **rhoE, const void **uvx
 int hydro_batch_copy_state(void *batch, int slot, void *rhoE, void *uvx, int to_host);
 /* Wait for every step enqueued on the batch. */
 int hydro_batch_sync(void *batch);
+/* Build (capture and instantiate) the graph of `nsteps` steps for the current instance set
+ * without running it, so that the next hydro_batch_run(nsteps) only launches. */
+int hydro_batch_prepare(void *batch, int nsteps);
 void hydro_batch_destroy(void *batch);
 
 /* The blast initial condition of hydro2d/main.cxx:280-338 (hydro3d/main.cxx:296-363) with

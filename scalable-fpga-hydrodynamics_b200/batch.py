@@ -92,6 +92,8 @@ def _declare(L):
     L.hydro_batch_destroy.restype = None
     L.hydro_batch_sync.argtypes = [vp]
     L.hydro_batch_sync.restype = _c.c_int
+    L.hydro_batch_prepare.argtypes = [vp, _c.c_int]
+    L.hydro_batch_prepare.restype = _c.c_int
     L._batch_declared = True
     return L
 
@@ -140,6 +142,10 @@ class Batch:
 
     def sync(self):
         _check(self.L.hydro_batch_sync(self.h))
+
+    def prepare(self, nsteps: int):
+        """Build the graph of `nsteps` steps now (the next run(nsteps) only launches)."""
+        _check(self.L.hydro_batch_prepare(self.h, nsteps))
 
     def status(self, slot: int) -> dict:
         s = BatchStatus()

@@ -313,6 +313,7 @@ class BatchBase {
     virtual size_t bytes(const hydro_blast_t &spec) const = 0;
     virtual int copy_state(int slot, void *rhoE, void *uvx, bool to_host) = 0;
     virtual int sync() = 0;
+    virtual int prepare(int nsteps) = 0;
 };
 
 template <class T, int D> class BatchEngine final : public BatchBase {
@@ -609,6 +610,15 @@ template <class T, int D> class BatchEngine final : public BatchBase {
         return kOk;
     }
 
+    int prepare(int nsteps) override
+    {
+        if (nsteps < 0) {
+            set_error(kErrArg, "batch prepare: negative step count");
+            return kErrArg;
+        }
+        return (dirty_ || nsteps != graph_steps_) ? rebuild(nsteps) : kOk;
+    }
+
     int sync() override
     {
         const cudaError_t e = cudaStreamSynchronize(stream_);
@@ -792,6 +802,12 @@ long long hydro_batch_bytes(void *b, const hydro_blast_t *spec)
 {
     if (!b || !spec) return kErrArg;
     return (long long)static_cast<BatchBase *>(b)->bytes(*spec);
+}
+
+int hydro_batch_prepare(void *b, int nsteps)
+{
+    if (!b) return kErrArg;
+    return static_cast<BatchBase *>(b)->prepare(nsteps);
 }
 
 int hydro_batch_sync(void *b)

@@ -42,9 +42,11 @@ class Record:
 
 
 def summarize(records, wall):
+    """Latency percentiles over the completed requests; throughput over all the work done
+    within the wall time (steps of unfinished requests included)."""
     done = [r for r in records if r.done is not None]
     tts = np.array([r.tts for r in done]) if done else np.array([np.nan])
-    work = sum(r.steps * r.cells for r in done)
+    work = sum(r.steps * r.cells for r in records)
     return dict(requests=len(records), completed=len(done), p50_s=float(np.percentile(tts, 50)),
                 p99_s=float(np.percentile(tts, 99)), mean_s=float(np.mean(tts)), wall_s=wall,
                 cell_updates=int(work), gcell_s=work / wall / 1e9 if wall > 0 else 0.0,
@@ -77,12 +79,13 @@ class Server:
             e.close()
         self.engines.clear()
 
-    def serve(self, requests, max_wall: float = None, keep_results: bool = False):
-        """Serve `requests` (workloads.Request) as they arrive; returns (records, wall
-        seconds). keep_results copies each retired request's final state to the host
-        (Record.status['state'])."""
+    def serve(self, requests, max_wall: float = None, keep_results: bool = False, dtype=None):
+        """Serve `requests` (workloads.Request) as they arrive, each in its own precision or
+        all in `dtype`; returns (records, wall seconds). keep_results copies each retired
+        request's final state to the host (Record.status['state'])."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        recs = {r.rid: Record(r.rid, r.arrival, dim=len(r.blast.nb), precision=np.dtype(r.dtype).name,
+        prec = lambda r: dtype or r.dtype
+        recs = {r.rid: Record(r.rid, r.arrival, dim=len(r.blast.nb), precision=np.dtype(prec(r)).name,
                               cells=int(np.prod(r.blast.nb))) for r in reqs}
         pending = deque()
         active = {}  # (key, slot) -> (request, bytes)
@@ -98,7 +101,7 @@ class Server:
             # admission, first come first served, while the state fits the budget
             while pending:
                 r = pending[0]
-                eng = self.engine(len(r.blast.nb), r.dtype)
+                eng = self.engine(len(r.blast.nb), prec(r))
                 need = eng.bytes(r.blast)
                 if need > self.budget:
                     pending.popleft()
@@ -108,7 +111,7 @@ class Server:
                     break
                 slot = eng.add(r.blast)
                 used += need
-                active[((len(r.blast.nb), np.dtype(r.dtype).name), slot)] = (r, need)
+                active[((len(r.blast.nb), np.dtype(prec(r)).name), slot)] = (r, need)
                 recs[r.rid].admit = clock()
                 pending.popleft()
             if not active:
@@ -134,20 +137,24 @@ class Server:
                     used -= need
                     del active[(k, slot)]
             if max_wall is not None and clock() > max_wall:
+                for (k, slot), (r, _need) in active.items():  # work done so far, unfinished
+                    recs[r.rid].steps = self.engines[k].status(slot)["steps"]
                 break
         wall = clock()
         return list(recs.values()), wall
 
 
-def serve_plain(requests, max_wall: float = None):
-    """First-come first-served, one request at a time through the plain path."""
+def serve_plain(requests, max_wall: float = None, dtype=None):
+    """First-come first-served, one request at a time through the plain path (in each
+    request's precision, or in `dtype` for all of them)."""
     torch = _torch()
     reqs = sorted(requests, key=lambda r: r.arrival)
     recs = []
     t0 = time.perf_counter()
     clock = lambda: time.perf_counter() - t0
     for r in reqs:
-        rec = Record(r.rid, r.arrival, dim=len(r.blast.nb), precision=np.dtype(r.dtype).name,
+        T = dtype or r.dtype
+        rec = Record(r.rid, r.arrival, dim=len(r.blast.nb), precision=np.dtype(T).name,
                      cells=int(np.prod(r.blast.nb)))
         recs.append(rec)
         if max_wall is not None and clock() > max_wall:
@@ -156,7 +163,7 @@ def serve_plain(requests, max_wall: float = None):
         if wait > 0:
             time.sleep(wait)
         rec.admit = clock()
-        run = BlastRun(r.blast.nb, r.dtype, blast=r.blast)
+        run = BlastRun(r.blast.nb, T, blast=r.blast)
         while run.t < r.blast.t_end and run.it < r.blast.max_steps:
             run.step()
             if max_wall is not None and clock() > max_wall:

@@ -61,12 +61,17 @@ def sound_crossing_time(p_out=0.1, rho=1.0, gamma=1.4, length=1.0):
     return length / math.sqrt(gamma * p_out / rho)
 
 
-def request_stream(rate: float, duration: float, seed: int = 0, frac_3d: float = 0.3, frac_fp64: float = 0.5,
-                   sides_2d=(128, 4096), sides_3d=(32, 256), t_end_frac=(0.05, 0.5)):
+def request_stream(rate: float, duration: float = math.inf, seed: int = 0, frac_3d: float = 0.3,
+                   frac_fp64: float = 0.5, sides_2d=(128, 4096), sides_3d=(32, 256), t_end_frac=(0.05, 0.5),
+                   count: int = None):
+    """Requests arriving within `duration` seconds, at most `count` of them (one of the two
+    must be finite)."""
+    if count is None and not math.isfinite(duration):
+        raise ValueError("request_stream needs a finite duration or a count")
     rng = np.random.default_rng(seed)
     out, t, rid = [], 0.0, 0
     tc = sound_crossing_time()
-    while True:
+    while count is None or len(out) < count:
         t += rng.exponential(1.0 / rate)
         if t > duration:
             break

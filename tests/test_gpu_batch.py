@@ -109,3 +109,65 @@ def test_batch_retire_remove_reuse(cuda):
     with pytest.raises(hb.HydroError):
         b.add(Blast(nb=(10, 10)))  # both slots in use
     b.close()
+
+
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+def test_batch3d_instance_equals_plain_path(cuda, T):
+    """A 3D blast through the 3D batch (beside two other instances) and through the plain
+    3D path: same t, same Dt, same interior bits."""
+    from hydro_b200.batch import Batch, Blast
+
+    nb = (40, 36, 30)
+    steps = 25
+    bl = Blast(nb=nb, max_steps=steps)
+    plain = hb.BlastRun(nb, T, blast=bl).run(1e9, steps)
+    b = Batch(3, T, capacity=4)
+    b.add(Blast(nb=(20, 50, 17), max_steps=steps + 3))
+    b.add(Blast(nb=(33, 12, 40), max_steps=4))
+    slot = b.add(bl)
+    b.run(steps + 3)
+    st = b.status(slot)
+    assert st["steps"] == steps and not st["active"]
+    assert st["t"] == plain.t
+    assert np.float64(st["dt"]) == np.float64(plain.dt)
+    ours = interior(b.state(slot), nb)
+    ref = interior(plain.host_state(), nb)
+    assert ours[0].tobytes() == ref[0].tobytes() and ours[1].tobytes() == ref[1].tobytes()
+    b.close()
+
+
+def test_batch3d_fp32_accuracy_vs_fp64_oracle(cuda, oracle):
+    """The reference 3D blast (24^3) through the FP32 3D batch against the FP64 oracle:
+    relative L1 on rho <= 1e-5."""
+    from hydro_b200.batch import Batch, Blast
+
+    nb = (24, 24, 24)
+    r64 = oracle.run(nb, np.float64, 2.0, 60)
+    b = Batch(3, np.float32, capacity=2)
+    s = b.add(Blast(nb=nb, t_end=2.0, max_steps=60))
+    b.run(60)
+    assert b.status(s)["steps"] == r64["it"]
+    a = interior(b.state(s), nb)[0][..., 0].astype(np.float64)
+    r = interior(r64["state"], nb)[0][..., 0]
+    l1 = np.abs(a - r).sum() / np.abs(r).sum()
+    print(f"batched 3D FP32 vs FP64 oracle: rho rel L1 {l1:.2e}")
+    assert l1 <= 1e-5
+    b.close()
+
+
+def test_autotune_picks_a_candidate(cuda, tmp_path, monkeypatch):
+    """The autotuner times every candidate chunk, caches the fastest per (GPU, dim,
+    precision) and `best_chunk` reads it back; an untuned key gives the default (0)."""
+    import json
+
+    import hydro_b200.autotune as at
+
+    monkeypatch.setattr(at, "CACHE", tmp_path / "tune.json")
+    assert at.best_chunk(2, np.float32) == 0
+    c = at.tune(2, np.float32, candidates=(64, 256), n=6, steps=3)
+    assert c in (64, 256)
+    assert at.best_chunk(2, np.float32) == c
+    entry = next(iter(json.loads((tmp_path / "tune.json").read_text()).values()))
+    assert set(entry["gcell_s"]) == {"64", "256"} and all(v > 0 for v in entry["gcell_s"].values())
+    c3 = at.tune(3, np.float64, candidates=(32, 64), n=4, steps=2)
+    assert c3 in (32, 64) and at.best_chunk(3, np.float64) == c3

@@ -1,0 +1,132 @@
+"""Host-side logic without a GPU: the seeded workloads, the serving summary, and the
+replica bookkeeping over a world of two gloo ranks on CPU."""
+from __future__ import annotations
+
+import math
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from conftest import load_pkg
+
+hb = load_pkg()
+
+
+def test_request_stream_needs_a_bound():
+    from hydro_b200.workloads import request_stream
+
+    with pytest.raises(ValueError):
+        request_stream(10.0)
+    a = request_stream(10.0, seed=4, count=12)
+    assert len(a) == 12 and all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
+    b = request_stream(10.0, duration=a[5].arrival + 1e-9, seed=4)
+    assert [r.rid for r in b] == list(range(6))
+    assert [r.blast.nb for r in b] == [r.blast.nb for r in a[:6]]
+
+
+def test_request_stream_distribution():
+    """Sides, dimensionality, precision and t_end follow the serving workload's ranges."""
+    from hydro_b200.workloads import request_stream, sound_crossing_time
+
+    reqs = request_stream(1000.0, seed=1, count=2000)
+    tc = sound_crossing_time()
+    n3 = sum(len(r.blast.nb) == 3 for r in reqs)
+    assert 0.25 < n3 / len(reqs) < 0.35
+    assert 0.45 < sum(r.dtype is np.float64 for r in reqs) / len(reqs) < 0.55
+    for r in reqs:
+        lo, hi = (32, 256) if len(r.blast.nb) == 3 else (64, 4096)
+        assert all(lo <= n <= hi for n in r.blast.nb), r.blast.nb
+        assert 0.05 * tc <= r.blast.t_end <= 0.5 * tc
+        ratio = r.blast.p_in / r.blast.p_out
+        assert 10 - 1e-9 <= ratio <= 1000 + 1e-9
+    gaps = np.diff([0.0] + [r.arrival for r in reqs])
+    assert abs(gaps.mean() - 1e-3) < 1e-4  # Poisson arrivals at the requested rate
+
+
+def test_batch_blasts_distribution():
+    from hydro_b200.workloads import batch_blasts
+
+    bl = batch_blasts(512, seed=2, steps=200)
+    for b in bl:
+        lo, hi = sorted(b.nb)
+        assert 32 <= lo and hi <= 2048 and hi / lo <= 2.0 + 1e-6
+        assert 0.05 * lo - 1e-9 <= b.radius <= 0.2 * lo + 1e-9
+        assert b.max_steps == 200 and b.rho_in == b.rho_out == 1.0 and b.gamma == 1.4
+        for c, n in zip(b.centre, b.nb):
+            assert 1 + 0.25 * (n - 1) - 1e-9 <= c <= 1 + 0.75 * (n - 1) + 1e-9
+
+
+def test_summarize_counts_partial_work():
+    from hydro_b200.serving import Record, summarize
+
+    recs = [Record(0, 0.0, done=1.0, steps=10, cells=100), Record(1, 0.5, done=3.5, steps=20, cells=50),
+            Record(2, 1.0, steps=7, cells=1000)]  # unfinished: counts as work, not latency
+    s = summarize(recs, wall=4.0)
+    assert s["completed"] == 2 and s["requests"] == 3
+    assert s["cell_updates"] == 10 * 100 + 20 * 50 + 7 * 1000
+    assert math.isclose(s["p50_s"], 2.0) and s["p99_s"] <= 3.0 + 1e-12
+    assert math.isclose(s["gcell_s"], 9000 / 4.0 / 1e9)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    try:
+        import importlib.util
+        import sys
+
+        from conftest import ROOT
+
+        spec = importlib.util.spec_from_file_location(
+            "hydro_b200_replicas", ROOT / "scalable-fpga-hydrodynamics_b200" / "replicas.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        reps = mod.Replicas("gloo", timeout_s=60)
+        reps.barrier()
+        mx = reps.max_over_ranks(10.0 * (rank + 1))
+        sm = reps.sum_over_ranks(rank + 1)
+        share = reps.share(range(11))
+        reps.barrier()
+        reps.close()
+        q.put((rank, mx, sm, share))
+    except Exception as e:  # reported to the parent
+        q.put((rank, repr(e), None, None))
+
+
+def test_replicas_gloo_two_ranks():
+    """Two ranks on CPU: max-over-ranks timing, the sum of work, and disjoint complete
+    shares of a request stream."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [o[1] for o in out] == [20.0, 20.0], out
+    assert [o[2] for o in out] == [3.0, 3.0]
+    shares = [o[3] for o in out]
+    assert sorted(shares[0] + shares[1]) == list(range(11)) and not set(shares[0]) & set(shares[1])
+
+
+def test_replicas_single_process_is_identity():
+    from hydro_b200.replicas import Replicas
+
+    r = Replicas("gloo", env={})
+    assert (r.rank, r.world) == (0, 1)
+    assert r.max_over_ranks(3.5) == 3.5 and r.share([1, 2, 3]) == [1, 2, 3]
+    r.barrier()
+    r.close()
