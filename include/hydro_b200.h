@@ -192,6 +192,8 @@ typedef struct hydro_batch_status {
     long long steps;
     int active;        /* 0 once t >= t_end, steps >= max_steps or an error */
     unsigned err;      /* bit 0: non-physical state; bit 1: a bounded wait timed out */
+    long long exact_passes; /* steps whose max signal speed needed the exact pass over all
+                               cells (no cell reached the skip threshold) */
 } hydro_batch_status_t;
 
 /* A batch of `dim`-D (2) instances in FP32 (precision_bytes 4) or FP64 (8), rows per work
@@ -218,6 +220,11 @@ int hydro_batch_sync(void *batch);
 /* Build (capture and instantiate) the graph of `nsteps` steps for the current instance set
  * without running it, so that the next hydro_batch_run(nsteps) only launches. */
 int hydro_batch_prepare(void *batch, int nsteps);
+/* The signal-speed skip of the batched step: a cell computes its exact signal speed only
+ * when an FP32 upper bound of it reaches `frac` x the previous step's max of its instance;
+ * a step where no cell does takes an exact pass over all the instance's cells. Dt is the
+ * exact value whatever `frac` is (default 0.9; 0 computes every cell exactly). */
+int hydro_batch_set_skip_fraction(void *batch, double frac);
 void hydro_batch_destroy(void *batch);
 
 /* The blast initial condition of hydro2d/main.cxx:280-338 (hydro3d/main.cxx:296-363) with

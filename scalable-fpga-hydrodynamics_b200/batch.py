@@ -29,7 +29,7 @@ class BatchStatus(_c.Structure):
 
     _fields_ = [("t", _c.c_double), ("dt", _c.c_double), ("mass", _c.c_double), ("mom", _c.c_double * 3),
                 ("energy", _c.c_double), ("max_speed", _c.c_double), ("steps", _c.c_longlong),
-                ("active", _c.c_int), ("err", _c.c_uint)]
+                ("active", _c.c_int), ("err", _c.c_uint), ("exact_passes", _c.c_longlong)]
 
 
 @dataclass
@@ -94,6 +94,8 @@ def _declare(L):
     L.hydro_batch_sync.restype = _c.c_int
     L.hydro_batch_prepare.argtypes = [vp, _c.c_int]
     L.hydro_batch_prepare.restype = _c.c_int
+    L.hydro_batch_set_skip_fraction.argtypes = [vp, _c.c_double]
+    L.hydro_batch_set_skip_fraction.restype = _c.c_int
     L._batch_declared = True
     return L
 
@@ -147,11 +149,16 @@ class Batch:
         """Build the graph of `nsteps` steps now (the next run(nsteps) only launches)."""
         _check(self.L.hydro_batch_prepare(self.h, nsteps))
 
+    def set_skip_fraction(self, frac: float):
+        """Signal-speed skip threshold as a fraction of the previous step's max (default
+        0.9; 0: every cell exact; above 1: every step takes the exact pass)."""
+        _check(self.L.hydro_batch_set_skip_fraction(self.h, float(frac)))
+
     def status(self, slot: int) -> dict:
         s = BatchStatus()
         _check(self.L.hydro_batch_status(self.h, slot, _c.byref(s)))
         return dict(t=s.t, dt=s.dt, mass=s.mass, mom=tuple(s.mom), energy=s.energy, max_speed=s.max_speed,
-                    steps=s.steps, active=bool(s.active), err=s.err)
+                    steps=s.steps, active=bool(s.active), err=s.err, exact_passes=s.exact_passes)
 
     def state(self, slot: int):
         """(rhoE, uvx) numpy arrays in the reference layout."""

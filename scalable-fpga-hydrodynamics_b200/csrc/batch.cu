@@ -38,6 +38,9 @@ template <class T> struct alignas(128) Inst2 {
     Phys<T> ph;
     T DX, DY, dt, DtDx, DtDy;
     double t, t_end;
+    double vmax_prev; // exact max signal speed of the previous step (0 before the first)
+    float ggm1;       // gamma * (gamma - 1) in FP32, for the signal-speed bound
+    long long exact_passes;
     long long ys;
     long long steps, max_steps;
     int nb_x, nb_y, nstrips, chunk;
@@ -50,6 +53,9 @@ template <class T> struct alignas(128) Inst3 {
     Phys<T> ph;
     T DX, DY, DZ, dt, DtDx, DtDy, DtDz;
     double t, t_end;
+    double vmax_prev; // exact max signal speed of the previous step (0 before the first)
+    float ggm1;       // gamma * (gamma - 1) in FP32, for the signal-speed bound
+    long long exact_passes;
     long long zs, zy;
     long long steps, max_steps;
     int nb_x, nb_y, nb_z, ntz, nty, chunk;
@@ -66,7 +72,7 @@ struct ItemPart {
 // per-slot status, host-mapped, written by the finalising item
 struct SlotStatus {
     double t, dt, sums[kSums], max_speed;
-    long long steps;
+    long long steps, exact_passes;
     int active;
     unsigned err;
 };
@@ -83,16 +89,20 @@ struct BatchAcc {
         c[q] = __dsub_rn(y, __dsub_rn(tt, s[q]));
         s[q] = tt;
     }
-    template <class T> __device__ __forceinline__ void add(T r, T mu, T mv, T mw, T E, T speed)
+    // conservation sums of one updated cell (the rho w sum stays 0 in 2D)
+    template <int D, class T> __device__ __forceinline__ void add_sums(T r, T mu, T mv, T mw, T E)
     {
         kahan(0, (double)r);
         kahan(1, (double)mu);
         kahan(2, (double)mv);
-        kahan(3, (double)mw);
+        if (D == 3) kahan(3, (double)mw);
         kahan(4, (double)E);
-        const double sp = (double)speed;
+        if (!(r > T(0))) err |= kErrNonPhysical;
+    }
+    __device__ __forceinline__ void add_speed(double sp)
+    {
         vmax = (sp > vmax) ? sp : vmax;
-        if (!(r > T(0)) || !(sp <= 1.0e300)) err |= kErrNonPhysical;
+        if (!(sp <= 1.0e300)) err |= kErrNonPhysical;
     }
 };
 
@@ -151,6 +161,56 @@ template <int NT> __device__ __forceinline__ void block_reduce(BatchAcc &a)
     __syncthreads();
 }
 
+// The signal-speed skip of the plain path, per instance: a cell computes its exact
+// speed only when its FP32 upper bound reaches kSkipFrac x the previous step's max.
+// skip_frac is kSkipFrac unless a caller set another fraction (0 turns the skip off;
+// above 1 every cell skips and every step takes the exact pass).
+template <class I> __device__ __forceinline__ float batch_threshold(const I *in, double skip_frac)
+{
+    return __double2float_rd(skip_frac * in->vmax_prev);
+}
+
+// Exact max signal speed over an instance's new state (the buffer the step wrote),
+// whole block; valid in thread 0. Runs only when every cell skipped the exact speed.
+template <int NT> __device__ __forceinline__ double block_max(double v, unsigned &err)
+{
+    __shared__ unsigned long long s_max[NT / 32];
+    const unsigned long long mb = block_max_bits<NT>((unsigned long long)__double_as_longlong(v), s_max);
+    if (__syncthreads_or(err != 0)) err = kErrNonPhysical;
+    return __longlong_as_double((long long)mb);
+}
+template <int NT, class T> __device__ double exact_max(const Inst2<T> *in, unsigned &err)
+{
+    const int b = in->parity ^ 1;
+    const T *r = in->rhoE[b], *u = in->uv[b];
+    const long long ny = in->nb_y, n = (long long)in->nb_x * ny;
+    double vmax = 0.0;
+    for (long long q = threadIdx.x; q < n; q += NT) {
+        const long long c = (1 + q / ny) * in->ys + 1 + q % ny;
+        const double sp = (double)speed2(__ldcg(r + 2 * c), __ldcg(u + 2 * c), __ldcg(u + 2 * c + 1),
+                                         __ldcg(r + 2 * c + 1), in->ph);
+        vmax = (sp > vmax) ? sp : vmax;
+        if (!(sp <= 1.0e300)) err = kErrNonPhysical;
+    }
+    return block_max<NT>(vmax, err);
+}
+template <int NT, class T> __device__ double exact_max(const Inst3<T> *in, unsigned &err)
+{
+    const int b = in->parity ^ 1;
+    const T *r = in->rhoE[b], *u = in->uvw[b];
+    const long long ncol = (long long)in->nb_y * in->nb_z, n = (long long)in->nb_x * ncol;
+    double vmax = 0.0;
+    for (long long q = threadIdx.x; q < n; q += NT) {
+        const long long rr = q % ncol;
+        const long long c = (1 + q / ncol) * in->zy + (1 + rr / in->nb_z) * in->zs + 1 + rr % in->nb_z;
+        const double sp = (double)speed3(__ldcg(r + 2 * c), __ldcg(u + 3 * c), __ldcg(u + 3 * c + 1),
+                                         __ldcg(u + 3 * c + 2), __ldcg(r + 2 * c + 1), in->ph);
+        vmax = (sp > vmax) ? sp : vmax;
+        if (!(sp <= 1.0e300)) err = kErrNonPhysical;
+    }
+    return block_max<NT>(vmax, err);
+}
+
 template <class T> __device__ __forceinline__ void set_dtdz(Inst2<T> *, T) {}
 template <class T> __device__ __forceinline__ void set_dtdz(Inst3<T> *in, T Dt) { in->DtDz = Ar<T>::div(Dt, in->DZ); }
 
@@ -168,6 +228,7 @@ template <class T, class I> __device__ __forceinline__ void advance(I *in, const
     in->DtDy = A::div(Dt, in->DY);
     set_dtdz<T>(in, Dt);
     in->parity ^= 1;
+    in->vmax_prev = a.vmax;
     in->err |= a.err;
     in->active = (in->t < in->t_end) && (in->steps < in->max_steps) && !(in->err & kErrNonPhysical);
     if (st) {
@@ -176,6 +237,7 @@ template <class T, class I> __device__ __forceinline__ void advance(I *in, const
         for (int q = 0; q < kSums; ++q) st->sums[q] = __dadd_rn(a.s[q], a.c[q]);
         st->max_speed = a.vmax;
         st->steps = in->steps;
+        st->exact_passes = in->exact_passes;
         st->active = in->active;
         st->err = in->err;
     }
@@ -185,7 +247,7 @@ template <class T, class I> __device__ __forceinline__ void advance(I *in, const
 
 // Merge an instance's item slots in item order and advance the instance (whole block).
 template <int NT, class T, class I>
-__device__ void finalize_instance(I *in, const ItemPart *parts, int nitems, SlotStatus *st)
+__device__ void finalize_instance(I *in, const ItemPart *parts, int nitems, SlotStatus *st, double skip_frac)
 {
     BatchAcc a;
     unsigned long long mb = 0ull;
@@ -198,6 +260,20 @@ __device__ void finalize_instance(I *in, const ItemPart *parts, int nitems, Slot
     }
     a.vmax = __longlong_as_double((long long)mb);
     block_reduce<NT>(a);
+    // cells whose speed bound was under the threshold skipped the exact speed; if no
+    // cell reached the threshold the skipped cells may hold the max: all cells again
+    __shared__ int s_redo;
+    if (threadIdx.x == 0) s_redo = (a.vmax < (double)batch_threshold(in, skip_frac)) ? 1 : 0;
+    __syncthreads();
+    if (s_redo) {
+        unsigned err = 0;
+        const double m = exact_max<NT, T>(in, err);
+        if (threadIdx.x == 0) {
+            a.vmax = m;
+            a.err |= err;
+            in->exact_passes += 1;
+        }
+    }
     if (threadIdx.x == 0) advance<T>(in, a, st);
 }
 
@@ -228,7 +304,7 @@ __device__ __forceinline__ bool publish_item(BatchAcc &acc, ItemPart *parts, int
 template <class T>
 __global__ void __launch_bounds__(kStripNT, 4) batch2d(Inst2<T> *insts, const int2 *items, const int2 *ranges,
                                                       int nitems, unsigned *counter, ItemPart *parts,
-                                                      SlotStatus *status)
+                                                      SlotStatus *status, double skip_frac)
 {
     __shared__ Smem2<T> S;
     __shared__ int s_item;
@@ -254,21 +330,25 @@ __global__ void __launch_bounds__(kStripNT, 4) batch2d(Inst2<T> *insts, const in
             prefetch_tensormap(&I->tm[par][1]);
         }
         BatchAcc acc;
+        const float tlof = batch_threshold(I, skip_frac), ggm1 = I->ggm1;
         const bool ok = march2d<T>(S, &I->tm[par][0], &I->tm[par][1], geo, I->rhoE[par ^ 1], I->uv[par ^ 1], ph,
                                    I->DtDx, I->DtDy, ld, [&](const Upd2<T> &o) {
-                                       acc.add(o.r, o.u, o.v, T(0), o.E, speed2(o.r, o.u, o.v, o.E, ph));
+                                       acc.add_sums<2>(o.r, o.u, o.v, T(0), o.E);
+                                       const float fu = (float)o.u, fv = (float)o.v;
+                                       const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1);
+                                       if (!(ub < tlof)) acc.add_speed((double)speed2(o.r, o.u, o.v, o.E, ph));
                                    });
         if (!ok) acc.err |= kErrWaitTimeout;
         const int2 rg = ranges[it.x];
         if (publish_item<kStripNT>(acc, parts, w, &I->done_items, rg.y, &s_last))
-            finalize_instance<kStripNT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr);
+            finalize_instance<kStripNT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
     }
 }
 
 template <class T>
 __global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *items, const int2 *ranges,
                                                   int nitems, unsigned *counter, ItemPart *parts,
-                                                  SlotStatus *status)
+                                                  SlotStatus *status, double skip_frac)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem3<T> &S = *reinterpret_cast<Smem3<T> *>(smem_raw);
@@ -291,13 +371,18 @@ __global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *
                          I->zs, I->zy};
         const Phys<T> ph = I->ph;
         BatchAcc acc;
+        const float tlof = batch_threshold(I, skip_frac), ggm1 = I->ggm1;
         march3d<T>(S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy,
                    I->DtDz, [&](const Upd3<T> &o) {
-                       acc.add(o.r, o.u, o.v, o.w, o.E, speed3(o.r, o.u, o.v, o.w, o.E, ph));
+                       acc.add_sums<3>(o.r, o.u, o.v, o.w, o.E);
+                       const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
+                       const float ub =
+                           speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1);
+                       if (!(ub < tlof)) acc.add_speed((double)speed3(o.r, o.u, o.v, o.w, o.E, ph));
                    });
         const int2 rg = ranges[it.x];
         if (publish_item<k3NT>(acc, parts, w, &I->done_items, rg.y, &s_last))
-            finalize_instance<k3NT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr);
+            finalize_instance<k3NT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
     }
 }
 
@@ -314,6 +399,7 @@ class BatchBase {
     virtual int copy_state(int slot, void *rhoE, void *uvx, bool to_host) = 0;
     virtual int sync() = 0;
     virtual int prepare(int nsteps) = 0;
+    virtual int set_skip_fraction(double f) = 0;
 };
 
 template <class T, int D> class BatchEngine final : public BatchBase {
@@ -435,6 +521,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
         I.ph.divgamma = T(one / I.ph.gm1);
         I.ph.K = T(s.K);
         I.ph.kneg = I.ph.K < T(0);
+        I.ggm1 = (float)I.ph.gamma * (float)I.ph.gm1;
         T first = 0;
         int rc;
         if constexpr (D == 2)
@@ -567,6 +654,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
         out->steps = v->steps;
         out->active = v->active;
         out->err = v->err;
+        out->exact_passes = v->exact_passes;
         return kOk;
     }
 
@@ -607,6 +695,17 @@ template <class T, int D> class BatchEngine final : public BatchBase {
             set_error(kErrCuda, "batch copy_state: %s", cudaGetErrorString(e));
             return kErrCuda;
         }
+        return kOk;
+    }
+
+    int set_skip_fraction(double f) override
+    {
+        if (!(f >= 0.0) || !(f <= 1e300)) {
+            set_error(kErrArg, "batch skip fraction: %g is not a finite non-negative number", f);
+            return kErrArg;
+        }
+        skip_frac_ = f;
+        dirty_ = true; // the fraction is a kernel argument of the captured graph
         return kOk;
     }
 
@@ -652,10 +751,10 @@ template <class T, int D> class BatchEngine final : public BatchBase {
     {
         if constexpr (D == 2)
             batch2d<T><<<blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
-                                                         status_d_);
+                                                         status_d_, skip_frac_);
         else
             batch3d<T><<<blocks_, k3NT, smem_, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
-                                                         status_d_);
+                                                         status_d_, skip_frac_);
     }
 
     // Work list and partial slots for the instances in use; the graph of `nsteps` steps.
@@ -716,6 +815,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
     }
 
     int chunk_, cap_;
+    double skip_frac_ = kSkipFrac;
     bool own_stream_ = false, dirty_ = true;
     cudaStream_t stream_ = nullptr;
     Inst *insts_ = nullptr;
@@ -808,6 +908,12 @@ int hydro_batch_prepare(void *b, int nsteps)
 {
     if (!b) return kErrArg;
     return static_cast<BatchBase *>(b)->prepare(nsteps);
+}
+
+int hydro_batch_set_skip_fraction(void *b, double frac)
+{
+    if (!b) return kErrArg;
+    return static_cast<BatchBase *>(b)->set_skip_fraction(frac);
 }
 
 int hydro_batch_sync(void *b)

@@ -171,3 +171,37 @@ def test_autotune_picks_a_candidate(cuda, tmp_path, monkeypatch):
     assert set(entry["gcell_s"]) == {"64", "256"} and all(v > 0 for v in entry["gcell_s"].values())
     c3 = at.tune(3, np.float64, candidates=(32, 64), n=4, steps=2)
     assert c3 in (32, 64) and at.best_chunk(3, np.float64) == c3
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("T", [np.float32, np.float64])
+def test_batch_speed_skip_never_changes_results(cuda, dim, T):
+    """The signal-speed skip is exact: with the skip off (fraction 0), at its default, and
+    with every cell skipping (every step after the first then takes the exact pass over
+    the instance), times, Dt, conservation sums and states are identical."""
+    from hydro_b200.batch import Batch
+    from hydro_b200.workloads import _blast, _sides
+
+    rng = np.random.default_rng(21 + dim)
+    lo, hi = (64, 200) if dim == 2 else (12, 40)
+    blasts = [_blast(rng, _sides(rng, lo, hi, dim), max_steps=12) for _ in range(5)]
+    steps = 12
+    runs = []
+    for frac in (0.0, 0.9, 1e30):
+        b = Batch(dim, T, capacity=8)
+        b.set_skip_fraction(frac)
+        slots = [b.add(bl) for bl in blasts]
+        b.run(steps)
+        runs.append(([b.status(s) for s in slots], [b.state(s) for s in slots]))
+        b.close()
+    for st_a, st_b in zip(runs[0][0], runs[2][0]):
+        assert st_a["exact_passes"] == 0 and st_b["exact_passes"] == steps - 1
+    for (stats, states) in runs[1:]:
+        for a, b2 in zip(runs[0][0], stats):
+            a, b2 = dict(a), dict(b2)
+            a.pop("exact_passes"), b2.pop("exact_passes")
+            assert a == b2
+        for (ra, ua), (rb, ub) in zip(runs[0][1], states):
+            assert ra.tobytes() == rb.tobytes() and ua.tobytes() == ub.tobytes()
+    with pytest.raises(hb.HydroError):
+        Batch(dim, T, capacity=1).set_skip_fraction(-1.0)
