@@ -8,16 +8,20 @@
 // is bit-identical to n plain steps in the same precision. 2D instances keep the pair
 // layout with rows padded to 16 bytes (TMA-fed); 3D instances keep the reference's
 // pair/triple layout (cp.async-fed). Work is a flat list of (instance, tile x chunk)
-// items; persistent blocks take items from an atomic counter. Every item writes its
-// partial sums (compensated FP64 mass, momenta and energy; max signal speed; error bits)
-// to its own slot; the item that completes an instance's step (ticket per instance)
-// merges that instance's slots in item order -- the result depends neither on which
-// block ran which item nor on the other instances in the batch -- and advances the
-// instance on the device:
+// items; persistent blocks take items from an atomic counter. Every item writes its max
+// signal speed and error bits to its own slot; the item that completes an instance's
+// step (ticket per instance) merges that instance's slots -- the result depends neither
+// on which block ran which item nor on the other instances in the batch -- and advances
+// the instance on the device:
 //   Dt = min(1e20, C_min / max_speed)   (hydro2d/kernel.cxx:318, main.cxx:706-781)
 //   t += Dt (FP64 accumulator), DtDx = Dt / DX ... (main.cxx:703-704, in T)
 //   active while t < t_end and steps < max_steps (main.cxx:689)
-// so a step needs no host round trip and n steps are captured as one CUDA graph.
+// so a step needs no host round trip and n steps are captured as one CUDA graph. The
+// graph ends with one pass over the final state that forms each instance's compensated
+// FP64 conservation sums (mass, momenta, energy) over the same items, merged per
+// instance in a fixed order (the step kernels carry no sums: fewer registers, more
+// resident blocks). The signal speed uses the plain path's exact skip (see
+// batch_threshold).
 #include <algorithm>
 #include <stdio.h>
 #include <string.h>
@@ -41,6 +45,7 @@ template <class T> struct alignas(128) Inst2 {
     double vmax_prev; // exact max signal speed of the previous step (0 before the first)
     float ggm1;       // gamma * (gamma - 1) in FP32, for the signal-speed bound
     long long exact_passes;
+    unsigned sum_items; // items of the end-of-run conservation sums done
     long long ys;
     long long steps, max_steps;
     int nb_x, nb_y, nstrips, chunk;
@@ -56,6 +61,7 @@ template <class T> struct alignas(128) Inst3 {
     double vmax_prev; // exact max signal speed of the previous step (0 before the first)
     float ggm1;       // gamma * (gamma - 1) in FP32, for the signal-speed bound
     long long exact_passes;
+    unsigned sum_items; // items of the end-of-run conservation sums done
     long long zs, zy;
     long long steps, max_steps;
     int nb_x, nb_y, nb_z, ntz, nty, chunk;
@@ -99,6 +105,17 @@ struct BatchAcc {
         kahan(4, (double)E);
         if (!(r > T(0))) err |= kErrNonPhysical;
     }
+    __device__ __forceinline__ void add_speed(double sp)
+    {
+        vmax = (sp > vmax) ? sp : vmax;
+        if (!(sp <= 1.0e300)) err |= kErrNonPhysical;
+    }
+};
+
+// What a step accumulates per cell: the max exact signal speed and error bits.
+struct MaxAcc {
+    double vmax = 0.0;
+    unsigned err = 0;
     __device__ __forceinline__ void add_speed(double sp)
     {
         vmax = (sp > vmax) ? sp : vmax;
@@ -215,11 +232,11 @@ template <class T> __device__ __forceinline__ void set_dtdz(Inst2<T> *, T) {}
 template <class T> __device__ __forceinline__ void set_dtdz(Inst3<T> *in, T Dt) { in->DtDz = Ar<T>::div(Dt, in->DZ); }
 
 // Time-step bookkeeping of one instance after its step (thread 0 of the finalising block).
-template <class T, class I> __device__ __forceinline__ void advance(I *in, const BatchAcc &a, SlotStatus *st)
+template <class T, class I> __device__ __forceinline__ void advance(I *in, double vmax, unsigned err, SlotStatus *st)
 {
     using A = Ar<T>;
     const T big = T(1e20);
-    const T dtn = A::div(in->ph.C_min, static_cast<T>(a.vmax));
+    const T dtn = A::div(in->ph.C_min, static_cast<T>(vmax));
     const T Dt = (dtn < big) ? dtn : big;
     in->steps += 1;
     in->t = __dadd_rn(in->t, (double)Dt);
@@ -228,14 +245,13 @@ template <class T, class I> __device__ __forceinline__ void advance(I *in, const
     in->DtDy = A::div(Dt, in->DY);
     set_dtdz<T>(in, Dt);
     in->parity ^= 1;
-    in->vmax_prev = a.vmax;
-    in->err |= a.err;
+    in->vmax_prev = vmax;
+    in->err |= err;
     in->active = (in->t < in->t_end) && (in->steps < in->max_steps) && !(in->err & kErrNonPhysical);
     if (st) {
         st->t = in->t;
         st->dt = (double)Dt;
-        for (int q = 0; q < kSums; ++q) st->sums[q] = __dadd_rn(a.s[q], a.c[q]);
-        st->max_speed = a.vmax;
+        st->max_speed = vmax;
         st->steps = in->steps;
         st->exact_passes = in->exact_passes;
         st->active = in->active;
@@ -245,36 +261,89 @@ template <class T, class I> __device__ __forceinline__ void advance(I *in, const
     in->done_items = 0;
 }
 
-// Merge an instance's item slots in item order and advance the instance (whole block).
-template <int NT, class T, class I>
-__device__ void finalize_instance(I *in, const ItemPart *parts, int nitems, SlotStatus *st, double skip_frac)
+// Block-wide max of a non-negative double and OR of error bits; valid in thread 0.
+template <int NT> __device__ __forceinline__ double block_max_err(double v, unsigned &err)
 {
-    BatchAcc a;
+    __shared__ unsigned long long s_max[NT / 32];
+    __shared__ unsigned s_err;
+    if (threadIdx.x == 0) s_err = 0u;
+    __syncthreads();
+    if (err) atomicOr(&s_err, err);
+    const unsigned long long mb = block_max_bits<NT>((unsigned long long)__double_as_longlong(v), s_max);
+    err = s_err;
+    __syncthreads(); // s_err / s_max free for the next use
+    return __longlong_as_double((long long)mb);
+}
+
+// Merge an instance's item maxima, take the exact pass if no cell reached the skip
+// threshold, and advance the instance (whole block).
+template <int NT, class T, class I>
+__device__ void finalize_step(I *in, const ItemPart *parts, int nitems, SlotStatus *st, double skip_frac)
+{
     unsigned long long mb = 0ull;
+    unsigned err = 0;
     for (int i = threadIdx.x; i < nitems; i += NT) {
-        const ItemPart &p = parts[i];
-        for (int q = 0; q < kSums; ++q) neumaier_merge(a.s[q], a.c[q], __ldcg(&p.s[q]), __ldcg(&p.c[q]));
-        const unsigned long long m = __ldcg(&p.maxbits);
+        const unsigned long long m = __ldcg(&parts[i].maxbits);
         mb = m > mb ? m : mb;
-        a.err |= __ldcg(&p.err);
+        err |= __ldcg(&parts[i].err);
     }
-    a.vmax = __longlong_as_double((long long)mb);
-    block_reduce<NT>(a);
+    double vmax = block_max_err<NT>(__longlong_as_double((long long)mb), err);
     // cells whose speed bound was under the threshold skipped the exact speed; if no
     // cell reached the threshold the skipped cells may hold the max: all cells again
     __shared__ int s_redo;
-    if (threadIdx.x == 0) s_redo = (a.vmax < (double)batch_threshold(in, skip_frac)) ? 1 : 0;
+    if (threadIdx.x == 0) s_redo = (vmax < (double)batch_threshold(in, skip_frac)) ? 1 : 0;
     __syncthreads();
     if (s_redo) {
-        unsigned err = 0;
-        const double m = exact_max<NT, T>(in, err);
+        unsigned e2 = 0;
+        const double m = exact_max<NT, T>(in, e2);
         if (threadIdx.x == 0) {
-            a.vmax = m;
-            a.err |= err;
+            vmax = m;
+            err |= e2;
             in->exact_passes += 1;
         }
     }
-    if (threadIdx.x == 0) advance<T>(in, a, st);
+    if (threadIdx.x == 0) advance<T>(in, vmax, err, st);
+}
+
+// Merge an instance's conservation-sum slots (fixed thread and lane order: the result
+// depends only on the instance) and publish them (whole block).
+template <int NT, class I>
+__device__ void finalize_sums(I *in, const ItemPart *parts, int nitems, SlotStatus *st)
+{
+    BatchAcc a;
+    for (int i = threadIdx.x; i < nitems; i += NT) {
+        const ItemPart &p = parts[i];
+        for (int q = 0; q < kSums; ++q) neumaier_merge(a.s[q], a.c[q], __ldcg(&p.s[q]), __ldcg(&p.c[q]));
+        a.err |= __ldcg(&p.err);
+    }
+    block_reduce<NT>(a);
+    if (threadIdx.x == 0) {
+        if (st)
+            for (int q = 0; q < kSums; ++q) st->sums[q] = __dadd_rn(a.s[q], a.c[q]);
+        __threadfence();
+        in->sum_items = 0;
+    }
+}
+
+// A step item's max and error bits into its slot; returns (in every thread) whether this
+// item completed its instance's step.
+template <int NT>
+__device__ __forceinline__ bool publish_step(const MaxAcc &acc, ItemPart *parts, int w, unsigned *done, int nitems,
+                                             int *s_last)
+{
+    unsigned err = acc.err;
+    const double vmax = block_max_err<NT>(acc.vmax, err);
+    if (threadIdx.x == 0) {
+        ItemPart &p = parts[w];
+        p.maxbits = (unsigned long long)__double_as_longlong(vmax);
+        p.err = err;
+        __threadfence();
+        *s_last = (atomicAdd(done, 1u) == (unsigned)nitems - 1u);
+    }
+    __syncthreads();
+    const bool last = *s_last != 0;
+    if (last) __threadfence();
+    return last;
 }
 
 // The item's partial sums into its slot; returns (in every thread) whether this item
@@ -301,8 +370,11 @@ __device__ __forceinline__ bool publish_item(BatchAcc &acc, ItemPart *parts, int
     return last;
 }
 
+// resident blocks per SM the register budget of the 2D step aims at
+template <class T> struct Batch2dOcc { static constexpr int value = sizeof(T) == 4 ? 5 : 4; };
+
 template <class T>
-__global__ void __launch_bounds__(kStripNT, 4) batch2d(Inst2<T> *insts, const int2 *items, const int2 *ranges,
+__global__ void __launch_bounds__(kStripNT, Batch2dOcc<T>::value) batch2d(Inst2<T> *insts, const int2 *items, const int2 *ranges,
                                                       int nitems, unsigned *counter, ItemPart *parts,
                                                       SlotStatus *status, double skip_frac)
 {
@@ -329,19 +401,19 @@ __global__ void __launch_bounds__(kStripNT, 4) batch2d(Inst2<T> *insts, const in
             prefetch_tensormap(&I->tm[par][0]);
             prefetch_tensormap(&I->tm[par][1]);
         }
-        BatchAcc acc;
+        MaxAcc acc;
         const float tlof = batch_threshold(I, skip_frac), ggm1 = I->ggm1;
         const bool ok = march2d<T>(S, &I->tm[par][0], &I->tm[par][1], geo, I->rhoE[par ^ 1], I->uv[par ^ 1], ph,
                                    I->DtDx, I->DtDy, ld, [&](const Upd2<T> &o) {
-                                       acc.add_sums<2>(o.r, o.u, o.v, T(0), o.E);
+                                       if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
                                        const float fu = (float)o.u, fv = (float)o.v;
                                        const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1);
                                        if (!(ub < tlof)) acc.add_speed((double)speed2(o.r, o.u, o.v, o.E, ph));
                                    });
         if (!ok) acc.err |= kErrWaitTimeout;
         const int2 rg = ranges[it.x];
-        if (publish_item<kStripNT>(acc, parts, w, &I->done_items, rg.y, &s_last))
-            finalize_instance<kStripNT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
+        if (publish_step<kStripNT>(acc, parts, w, &I->done_items, rg.y, &s_last))
+            finalize_step<kStripNT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
     }
 }
 
@@ -370,19 +442,73 @@ __global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *
         const March3 geo{k3TZ * tz, k3TY * ty, i0, min(i0 + I->chunk - 1, I->nb_x), I->nb_x, I->nb_y, I->nb_z,
                          I->zs, I->zy};
         const Phys<T> ph = I->ph;
-        BatchAcc acc;
+        MaxAcc acc;
         const float tlof = batch_threshold(I, skip_frac), ggm1 = I->ggm1;
         march3d<T>(S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy,
                    I->DtDz, [&](const Upd3<T> &o) {
-                       acc.add_sums<3>(o.r, o.u, o.v, o.w, o.E);
+                       if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
                        const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
                        const float ub =
                            speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1);
                        if (!(ub < tlof)) acc.add_speed((double)speed3(o.r, o.u, o.v, o.w, o.E, ph));
                    });
         const int2 rg = ranges[it.x];
-        if (publish_item<k3NT>(acc, parts, w, &I->done_items, rg.y, &s_last))
-            finalize_instance<k3NT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
+        if (publish_step<k3NT>(acc, parts, w, &I->done_items, rg.y, &s_last))
+            finalize_step<k3NT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
+    }
+}
+
+// End-of-run conservation sums (compensated FP64 mass, momenta, energy) of every instance
+// over the same work items: one pass over the current state after the run's last step.
+template <int NT, class T> __device__ __forceinline__ void sum_item(const Inst2<T> *I, int y, BatchAcc &acc)
+{
+    using V2 = typename Vec2<T>::type;
+    const int strip = y % I->nstrips, ck = y / I->nstrips;
+    const int t = threadIdx.x, j = kStripW * strip + t;
+    if (t < 1 || t > kStripW || j > I->nb_y) return;
+    const int i0 = 1 + ck * I->chunk, i1 = min(i0 + I->chunk - 1, I->nb_x);
+    const V2 *r = reinterpret_cast<const V2 *>(I->rhoE[I->parity]);
+    const V2 *u = reinterpret_cast<const V2 *>(I->uv[I->parity]);
+    for (int i = i0; i <= i1; ++i) {
+        const long long c = (long long)i * I->ys + j;
+        const V2 a = r[c], b = u[c];
+        acc.add_sums<2>(a.x, b.x, b.y, T(0), a.y);
+    }
+}
+template <int NT, class T> __device__ __forceinline__ void sum_item(const Inst3<T> *I, int y, BatchAcc &acc)
+{
+    const int tz = y % I->ntz, rem = y / I->ntz;
+    const int ty = rem % I->nty, ck = rem / I->nty;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int k = k3TZ * tz + lane, j = k3TY * ty + w;
+    if (w < 1 || w > k3TY || lane < 1 || lane > k3TZ || j > I->nb_y || k > I->nb_z) return;
+    const int i0 = 1 + ck * I->chunk, i1 = min(i0 + I->chunk - 1, I->nb_x);
+    const T *r = I->rhoE[I->parity], *u = I->uvw[I->parity];
+    for (int i = i0; i <= i1; ++i) {
+        const long long c = (long long)i * I->zy + (long long)j * I->zs + k;
+        acc.add_sums<3>(r[2 * c], u[3 * c], u[3 * c + 1], u[3 * c + 2], r[2 * c + 1]);
+    }
+}
+
+template <int NT, class T, class I>
+__global__ void __launch_bounds__(NT) batch_sums(I *insts, const int2 *items, const int2 *ranges, int nitems,
+                                                 unsigned *counter, ItemPart *parts, SlotStatus *status)
+{
+    __shared__ int s_item;
+    __shared__ int s_last;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int w = s_item;
+        if (w >= nitems) break;
+        const int2 it = items[w];
+        I *in = insts + it.x;
+        BatchAcc acc;
+        sum_item<NT, T>(in, it.y, acc);
+        const int2 rg = ranges[it.x];
+        if (publish_item<NT>(acc, parts, w, &in->sum_items, rg.y, &s_last))
+            finalize_sums<NT>(in, parts + rg.x, rg.y, status ? status + it.x : nullptr);
     }
 }
 
@@ -433,6 +559,14 @@ template <class T, int D> class BatchEngine final : public BatchBase {
             if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch3d<T>, k3NT, smem_);
         }
         blocks_ = nsm * std::max(1, occ);
+        int occ_s = 0;
+        if (e == cudaSuccess) {
+            if constexpr (D == 2)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, batch_sums<kStripNT, T, Inst>, kStripNT, 0);
+            else
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, batch_sums<k3NT, T, Inst>, k3NT, 0);
+        }
+        sum_blocks_ = nsm * std::max(1, occ_s);
         slots_.resize(cap_);
         host_ranges_.assign(cap_, make_int2(0, 0));
         *rc = (e == cudaSuccess) ? kOk : kErrCuda;
@@ -757,7 +891,18 @@ template <class T, int D> class BatchEngine final : public BatchBase {
                                                          status_d_, skip_frac_);
     }
 
-    // Work list and partial slots for the instances in use; the graph of `nsteps` steps.
+    void launch_sums()
+    {
+        if constexpr (D == 2)
+            batch_sums<kStripNT, T, Inst><<<sum_blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_,
+                                                                                counter_ + 1, parts_, status_d_);
+        else
+            batch_sums<k3NT, T, Inst><<<sum_blocks_, k3NT, 0, stream_>>>(insts_, items_, ranges_, nitems_,
+                                                                        counter_ + 1, parts_, status_d_);
+    }
+
+    // Work list and partial slots for the instances in use; the graph of `nsteps` steps
+    // followed by the conservation sums.
     int rebuild(int nsteps)
     {
         std::vector<int2> items;
@@ -800,6 +945,12 @@ template <class T, int D> class BatchEngine final : public BatchBase {
                     e = cudaGetLastError();
                 }
             }
+            // the conservation sums of the state the run ends on
+            if (e == cudaSuccess) e = cudaMemsetAsync(counter_ + 1, 0, sizeof(unsigned), stream_);
+            if (e == cudaSuccess) {
+                launch_sums();
+                e = cudaGetLastError();
+            }
             const cudaError_t e2 = cudaStreamEndCapture(stream_, &g);
             if (e == cudaSuccess) e = e2;
             if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_, g, 0);
@@ -827,7 +978,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
     SlotStatus *status_h_ = nullptr, *status_d_ = nullptr;
     std::vector<Slot> slots_;
     std::vector<int2> host_ranges_;
-    int nitems_ = 0, blocks_ = 148, graph_steps_ = -1, smem_ = 0;
+    int nitems_ = 0, blocks_ = 148, sum_blocks_ = 148, graph_steps_ = -1, smem_ = 0;
     cudaGraphExec_t graph_ = nullptr;
 };
 
