@@ -283,11 +283,12 @@ def cpu_reference_sample(nb_y: int, rows: int, seconds: float, threads: int):
 
 
 # --------------------------------------------------------------- batched / serving ---
-def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, log=print):
+def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=0, log=print):
     """The batched workload (256 seeded 2D blasts, sides log-uniform in [64, 2048], 200
     steps each) through the FP32 and FP64 batch engines (chunk from the autotuner), and the
     same instances one at a time through the plain FP64 path. Accuracy: FP32 against the
-    FP64 batch (bit-identical to the plain FP64 path) on every instance."""
+    FP64 batch (bit-identical to the plain FP64 path) on every instance. `chunk` > 0 fixes
+    the rows per work item instead of asking the autotuner."""
     from hydro_b200.autotune import tune
     from hydro_b200.batch import Batch
     from hydro_b200.workloads import batch_blasts
@@ -297,15 +298,15 @@ def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, log=pr
     cells = sum(int(np.prod(b.nb)) for b in blasts)
     states = {}
     for T in (np.float32, np.float64):
-        chunk = tune(2, T, log=log)
+        ck = chunk if chunk > 0 else tune(2, T, log=log)
         s = torch.cuda.Stream()
         # warm-up: a throw-away batch of the same instances runs a few steps
-        w = Batch(2, T, chunk=chunk, capacity=n, stream=s)
+        w = Batch(2, T, chunk=ck, capacity=n, stream=s)
         for bl in blasts[:32]:
             w.add(bl)
         w.run(3)
         w.close()
-        b = Batch(2, T, chunk=chunk, capacity=n, stream=s)
+        b = Batch(2, T, chunk=ck, capacity=n, stream=s)
         slots = [b.add(bl) for bl in blasts]
         b.prepare(steps)  # graph captured and instantiated outside the timed region
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -321,7 +322,7 @@ def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, log=pr
         assert done == n * steps, (done, n * steps)
         key = "fp32" if T is np.float32 else "fp64"
         out[f"batched_{key}"] = dict(value=cells * steps / (ms / 1e3) / 1e9, unit=UNIT, ms=ms, wall_s=wall,
-                                     chunk=chunk, instances=n, steps=steps, cells=cells,
+                                     chunk=ck, instances=n, steps=steps, cells=cells,
                                      bytes_per_cell=32 if T is np.float32 else 64)
         states[key] = [b.state(k)[0] for k in slots]
         b.close()
@@ -409,6 +410,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-instances", type=int, default=256)
+    ap.add_argument("--batched-steps", type=int, default=200)
+    ap.add_argument("--batched-chunk", type=int, default=0, help="rows per work item (0: autotuned)")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-rates", type=float, nargs="+", default=[10.0, 1000.0])
     ap.add_argument("--serving-requests", type=int, default=8)
@@ -513,7 +517,8 @@ def main():
     batched = serving = None
     if rank == 0 and world == 1 and not args.no_batched and args.case == "2d_f64":
         barrier()
-        batched = bench_batched(hb, torch, log=log)
+        batched = bench_batched(hb, torch, n=args.batched_instances, steps=args.batched_steps,
+                                chunk=args.batched_chunk, log=log)
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.no_serving and args.case == "2d_f64":
         serving = bench_serving(hb, torch, rates=tuple(args.serving_rates), nreq=args.serving_requests,
