@@ -70,8 +70,8 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
-        self.idx = gpu_index
+    def __init__(self, gpu: str):
+        self.idx = gpu  # nvidia-smi -i accepts an index or a GPU UUID
         self.proc = None
         self.path = None
 
@@ -115,14 +115,56 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def gpu_uuid(torch, index):
+    """The NVML / nvidia-smi name of CUDA device `index` (robust to CUDA_VISIBLE_DEVICES)."""
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(index).uuid)
+    except Exception:
+        return str(index)
+
+
+class EnergyMeter:
+    """GPU energy from NVML's total-energy counter (millijoules since driver load), read
+    before and after a region. Read-only; None where NVML or the counter is missing."""
+
+    def __init__(self, uuid: str):
+        self.h = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = (pynvml.nvmlDeviceGetHandleByUUID(uuid) if uuid.startswith("GPU-")
+                      else pynvml.nvmlDeviceGetHandleByIndex(int(uuid)))
+        except Exception:
+            self.h = None
+
+    def read(self):
+        if self.h is None:
+            return None
+        try:
+            return self.nv.nvmlDeviceGetTotalEnergyConsumption(self.h) / 1e3
+        except Exception:
+            return None
+
+
+def energy_entry(joules, seconds, cell_updates):
+    if joules is None or seconds <= 0:
+        return None
+    return dict(joules=joules, avg_w=joules / seconds, nj_per_cell_update=joules / cell_updates * 1e9,
+                source="NVML total energy counter around the timed region")
+
+
 # -------------------------------------------------------------- GPU measurements ---
-def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0):
+def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0, meter=None):
     """Host loop with the state resident on the device; CUDA events on the launching
-    stream: total time of `steps` steps and per-step kernel time."""
+    stream: total time of `steps` steps and per-step kernel time (and the energy of the
+    timed steps when a meter is given)."""
     run = hb.BlastRun(nb, T, kernel=kernel)
     for _ in range(warmup):
         run.step()
     torch.cuda.synchronize()
+    j0 = meter.read() if meter else None
     stream = torch.cuda.current_stream()
     E = torch.cuda.Event
     e_start, e_end = E(enable_timing=True), E(enable_timing=True)
@@ -135,12 +177,14 @@ def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0):
         run.step_finish()
     e_end.record(stream)
     torch.cuda.synchronize()
+    j1 = meter.read() if meter else None
     total_ms = e_start.elapsed_time(e_end)
     kern_ms = [a.elapsed_time(b) for a, b in per]
     info = run.last_info
     # an asynchronous step launches the update kernel and the signal-speed check kernel
     # (which returns at once unless the fused maximum fell under its skip threshold)
-    res = dict(total_ms=total_ms, kernel_ms=kern_ms, kernel=int(info.kernel), it=run.it, launches_per_step=2)
+    res = dict(total_ms=total_ms, kernel_ms=kern_ms, kernel=int(info.kernel), it=run.it, launches_per_step=2,
+               energy_j=(j1 - j0) if (j0 is not None and j1 is not None) else None)
     del run
     torch.cuda.empty_cache()
     return res
@@ -283,7 +327,7 @@ def cpu_reference_sample(nb_y: int, rows: int, seconds: float, threads: int):
 
 
 # --------------------------------------------------------------- batched / serving ---
-def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=0, log=print):
+def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=0, log=print, meter=None):
     """The batched workload (256 seeded 2D blasts, sides log-uniform in [64, 2048], 200
     steps each) through the FP32 and FP64 batch engines (chunk from the autotuner), and the
     same instances one at a time through the plain FP64 path. Accuracy: FP32 against the
@@ -311,19 +355,23 @@ def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=
         b.prepare(steps)  # graph captured and instantiated outside the timed region
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        j0 = meter.read() if meter else None
         t0 = time.perf_counter()
         e0.record(s)
         b.run(steps, sync=False)
         e1.record(s)
         b.sync()
         wall = time.perf_counter() - t0
+        j1 = meter.read() if meter else None
         ms = e0.elapsed_time(e1)
         done = sum(b.status(k)["steps"] for k in slots)
         assert done == n * steps, (done, n * steps)
         key = "fp32" if T is np.float32 else "fp64"
         out[f"batched_{key}"] = dict(value=cells * steps / (ms / 1e3) / 1e9, unit=UNIT, ms=ms, wall_s=wall,
                                      chunk=ck, instances=n, steps=steps, cells=cells,
-                                     bytes_per_cell=32 if T is np.float32 else 64)
+                                     bytes_per_cell=32 if T is np.float32 else 64,
+                                     energy=energy_entry(None if j0 is None or j1 is None else j1 - j0, wall,
+                                                         cells * steps))
         states[key] = [b.state(k)[0] for k in slots]
         b.close()
     # accuracy of the FP32 batch against FP64 (rho, relative L1 and L-inf per instance)
@@ -469,9 +517,11 @@ def main():
     kname = f"strip{dim}d<{'double' if isz == 8 else 'float'}>"
 
     barrier()
-    sampler = ClockSampler(local)
+    uuid = gpu_uuid(torch, local)
+    meter = EnergyMeter(uuid)
+    sampler = ClockSampler(uuid)
     sampler.start()
-    r = bench_resident(hb, torch, nb, Tcase, args.steps, args.warmup)
+    r = bench_resident(hb, torch, nb, Tcase, args.steps, args.warmup, meter=meter)
     clocks = sampler.stop()
     barrier()
     total_ms = max_over_ranks(r["total_ms"])
@@ -518,7 +568,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_batched and args.case == "2d_f64":
         barrier()
         batched = bench_batched(hb, torch, n=args.batched_instances, steps=args.batched_steps,
-                                chunk=args.batched_chunk, log=log)
+                                chunk=args.batched_chunk, log=log, meter=meter)
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.no_serving and args.case == "2d_f64":
         serving = bench_serving(hb, torch, rates=tuple(args.serving_rates), nreq=args.serving_requests,
@@ -540,7 +590,8 @@ def main():
                                 l2=f"inputs larger than L2 ({cells * bpc / 2 / 1e9:.1f} GB state, 126 MB L2)",
                                 parallelism=f"replicas x{world}"),
                     roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps * r["launches_per_step"],
-                    clocks=clocks, variants=variants, batched=batched, serving=serving)
+                    clocks=clocks, energy=energy_entry(r["energy_j"], total_ms / 1e3, cells * args.steps),
+                    variants=variants, batched=batched, serving=serving)
         print(json.dumps(line), flush=True)
     reps.barrier()
     reps.close()
