@@ -52,21 +52,25 @@ struct March3 {
     long long zs, zy; // strides in cells of a Y row and of an X plane
 };
 
-template <class T, class Sink>
-__device__ __forceinline__ void march3d(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
-                                        const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &&sink)
+// kEdge = false: a tile whose every lane holds a real cell (1 <= j <= NB_Y,
+// 1 <= k <= NB_Z) and whose faces used by interior lanes touch no wall; it needs neither
+// the unit-state substitution nor the wall mirrors. kEdge = true: any tile.
+template <bool kEdge, class T, class Sink>
+__device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
+                                             const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &sink)
 {
     constexpr unsigned FULL = 0xffffffffu;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int k = g.kbase + lane, j = g.jbase + w;
     const int nplanes = g.i1 - g.i0 + 3;
-    const bool in_array = (j <= g.nb_y + 1) && (k <= g.nb_z + 1);
-    const bool interior = (w >= 1) && (w <= k3TY) && (lane >= 1) && (lane <= k3TZ) && (j <= g.nb_y) && (k <= g.nb_z);
-    const bool iwarp = (w >= 1) && (w <= k3TY) && (g.jbase + 1 <= g.nb_y); // warp holds interior rows
+    const bool in_array = !kEdge || ((j <= g.nb_y + 1) && (k <= g.nb_z + 1));
+    const bool interior =
+        (w >= 1) && (w <= k3TY) && (lane >= 1) && (lane <= k3TZ) && (!kEdge || ((j <= g.nb_y) && (k <= g.nb_z)));
+    const bool iwarp = (w >= 1) && (w <= k3TY) && (!kEdge || (g.jbase + 1 <= g.nb_y)); // warp holds interior rows
     const long long colofs = (long long)j * g.zs + k;
     // ghost cells (j or k = 0 or NB+1) and cells past the array are never used: they
     // convert a unit state so every lane's reciprocal / square root stays regular
-    const bool real = (j >= 1) && (j <= g.nb_y) && (k >= 1) && (k <= g.nb_z);
+    const bool real = !kEdge || ((j >= 1) && (j <= g.nb_y) && (k >= 1) && (k <= g.nb_z));
 
     __syncthreads(); // the previous march of this block is done with the exchange buffers
     auto issue = [&](int m) {
@@ -94,9 +98,13 @@ __device__ __forceinline__ void march3d(Smem3<T> &S, const T *rhoE, const T *uvw
         issue(m + k3Stages - 1);
         cp_async_wait<k3Stages - 1>();
         const int s = m % k3Stages;
-        const T ur = real ? S.st[s][0][t] : T(1), uE = real ? S.st[s][1][t] : T(1);
-        const T uu = real ? S.st[s][2][t] : T(0), uv = real ? S.st[s][3][t] : T(0);
-        const T uw = real ? S.st[s][4][t] : T(0);
+        T ur = S.st[s][0][t], uE = S.st[s][1][t];
+        T uu = S.st[s][2][t], uv = S.st[s][3][t], uw = S.st[s][4][t];
+        if (kEdge && !real) {
+            ur = T(1);
+            uE = T(1);
+            uu = uv = uw = T(0);
+        }
         const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, ph);
         {
             const FaceIn3<T> fy = face3_y(P);
@@ -118,8 +126,10 @@ __device__ __forceinline__ void march3d(Smem3<T> &S, const T *rhoE, const T *uvw
                 FaceIn3<T> nb{x[0 * k3NT], x[1 * k3NT], x[2 * k3NT], x[3 * k3NT], x[4 * k3NT],
                               x[5 * k3NT], x[6 * k3NT], x[7 * k3NT], x[8 * k3NT]};
                 FaceIn3<T> L = me, R = nb;
-                if (j == 0) L = mirror3(nb);
-                if (j == g.nb_y) R = mirror3(me);
+                if (kEdge) {
+                    if (j == 0) L = mirror3(nb);
+                    if (j == g.nb_y) R = mirror3(me);
+                }
                 fy = face_flux3(L, R, ph);
                 T *xf = &S.xF[m & 1][0][t];
                 xf[0 * k3NT] = fy.r; xf[1 * k3NT] = fy.n; xf[2 * k3NT] = fy.t1; xf[3 * k3NT] = fy.t2;
@@ -140,8 +150,10 @@ __device__ __forceinline__ void march3d(Smem3<T> &S, const T *rhoE, const T *uvw
                 nz.mt2 = __shfl_down_sync(FULL, mz.mt2, 1);
                 nz.eup = __shfl_down_sync(FULL, mz.eup, 1);
                 FaceIn3<T> L = mz, R = nz;
-                if (k == 0) L = mirror3(nz);
-                if (k == g.nb_z) R = mirror3(mz);
+                if (kEdge) {
+                    if (k == 0) L = mirror3(nz);
+                    if (k == g.nb_z) R = mirror3(mz);
+                }
                 fz = face_flux3(L, R, ph);
             }
             __syncthreads(); // +y faces of this plane published
@@ -174,6 +186,20 @@ __device__ __forceinline__ void march3d(Smem3<T> &S, const T *rhoE, const T *uvw
         Ur = ur; Uu = uu; Uv = uv; Uw = uw; UE = uE;
     }
     cp_async_wait<0>();
+}
+
+// One tile march: the lean form for tiles away from walls and ghosts, the general one
+// elsewhere (the choice is uniform over the block).
+template <class T, class Sink>
+__device__ __forceinline__ void march3d(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
+                                        const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &&sink)
+{
+    const bool inner =
+        g.jbase >= 1 && g.jbase + k3Warps - 1 <= g.nb_y && g.kbase >= 1 && g.kbase + 31 <= g.nb_z;
+    if (inner)
+        march3d_tile<false>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
+    else
+        march3d_tile<true>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
 }
 
 } // namespace hydro
