@@ -58,11 +58,13 @@ struct March2 {
     long long ys;
 };
 
-// Returns false when a bounded barrier wait gave up (the block then stops marching).
-template <class T, class Sink>
-__device__ __forceinline__ bool march2d(Smem2<T> &S, const CUtensorMap *tmr, const CUtensorMap *tmu, const March2 &g,
-                                        T *rhoE_n, T *uv_n, const Phys<T> &ph, T DtDx, T DtDy, unsigned &ld,
-                                        Sink &&sink)
+// kEdge = false: a strip whose every lane holds a real column (1 <= j <= NB_Y), so no
+// unit-state substitution and no wall face that an interior lane uses; kEdge = true: any
+// strip. Returns false when a bounded barrier wait gave up (the block then stops).
+template <bool kEdge, class T, class Sink>
+__device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tmr, const CUtensorMap *tmu,
+                                              const March2 &g, T *rhoE_n, T *uv_n, const Phys<T> &ph, T DtDx,
+                                              T DtDy, unsigned &ld, Sink &sink)
 {
     using V2 = typename Vec2<T>::type;
     constexpr unsigned FULL = 0xffffffffu;
@@ -70,10 +72,10 @@ __device__ __forceinline__ bool march2d(Smem2<T> &S, const CUtensorMap *tmr, con
     const int t = threadIdx.x;
     const int j = g.jbase + t;
     const int nrows = g.i1 - g.i0 + 3; // with one halo row above and below
-    const bool interior = (t >= 1) && (t <= kStripW) && (j <= g.nb_y);
+    const bool interior = (t >= 1) && (t <= kStripW) && (!kEdge || j <= g.nb_y);
     const int xcoord = 2 * g.jbase;
     // the two wall faces live in at most two warps; the others skip the mirror selects
-    const bool wall_warp = __any_sync(FULL, j == 0 || j == g.nb_y);
+    const bool wall_warp = kEdge && __any_sync(FULL, j == 0 || j == g.nb_y);
     // lanes whose column is a ghost (j = 0, j = NB_Y+1) or past the array hold zeros;
     // their primitives are never used, so they convert a unit state instead (keeps the
     // reciprocal / square root of every lane on its regular path)
@@ -101,7 +103,7 @@ __device__ __forceinline__ bool march2d(Smem2<T> &S, const CUtensorMap *tmr, con
         const int s = q % kStages;
         if (!mbar_wait_bounded(&S.full[s], (q / kStages) & 1)) S.abort = 1;
         V2 a = S.sr[s][t], b = S.su[s][t];
-        if (!real_col) {
+        if (kEdge && !real_col) {
             a = mk2<T>(T(1), T(1));
             b = mk2<T>(T(0), T(0));
         }
@@ -161,6 +163,18 @@ __device__ __forceinline__ bool march2d(Smem2<T> &S, const CUtensorMap *tmr, con
         return false;
     }
     return true;
+}
+
+// One strip march: the lean form away from the Y walls, the general one at them (the
+// choice is uniform over the block).
+template <class T, class Sink>
+__device__ __forceinline__ bool march2d(Smem2<T> &S, const CUtensorMap *tmr, const CUtensorMap *tmu, const March2 &g,
+                                        T *rhoE_n, T *uv_n, const Phys<T> &ph, T DtDx, T DtDy, unsigned &ld,
+                                        Sink &&sink)
+{
+    if (g.jbase >= 1 && g.jbase + kStripNT - 1 <= g.nb_y)
+        return march2d_strip<false>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
+    return march2d_strip<true>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
 }
 
 } // namespace hydro
