@@ -43,7 +43,7 @@ template <class T> struct alignas(128) Inst2 {
     T DX, DY, dt, DtDx, DtDy;
     double t, t_end;
     double vmax_prev; // exact max signal speed of the previous step (0 before the first)
-    float ggm1;       // gamma * (gamma - 1) in FP32, for the signal-speed bound
+    float ggm1;       // gamma * (gamma - 1), for the signal-speed skip test
     long long exact_passes;
     unsigned sum_items; // items of the end-of-run conservation sums done
     long long ys;
@@ -59,7 +59,7 @@ template <class T> struct alignas(128) Inst3 {
     T DX, DY, DZ, dt, DtDx, DtDy, DtDz;
     double t, t_end;
     double vmax_prev; // exact max signal speed of the previous step (0 before the first)
-    float ggm1;       // gamma * (gamma - 1) in FP32, for the signal-speed bound
+    float ggm1;       // gamma * (gamma - 1), for the signal-speed skip test
     long long exact_passes;
     unsigned sum_items; // items of the end-of-run conservation sums done
     long long zs, zy;
@@ -402,13 +402,13 @@ __global__ void __launch_bounds__(kStripNT, Batch2dOcc<T>::value) batch2d(Inst2<
             prefetch_tensormap(&I->tm[par][1]);
         }
         MaxAcc acc;
-        const float tlof = batch_threshold(I, skip_frac), ggm1 = I->ggm1;
+        const float tlo2 = skip_tlo2(batch_threshold(I, skip_frac)), ggm1 = I->ggm1;
         const bool ok = march2d<T>(S, &I->tm[par][0], &I->tm[par][1], geo, I->rhoE[par ^ 1], I->uv[par ^ 1], ph,
                                    I->DtDx, I->DtDy, ld, [&](const Upd2<T> &o) {
                                        if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
                                        const float fu = (float)o.u, fv = (float)o.v;
-                                       const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1);
-                                       if (!(ub < tlof)) acc.add_speed((double)speed2(o.r, o.u, o.v, o.E, ph));
+                                       if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1, tlo2))
+                                           acc.add_speed((double)speed2(o.r, o.u, o.v, o.E, ph));
                                    });
         if (!ok) acc.err |= kErrWaitTimeout;
         const int2 rg = ranges[it.x];
@@ -443,14 +443,13 @@ __global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *
                          I->zs, I->zy};
         const Phys<T> ph = I->ph;
         MaxAcc acc;
-        const float tlof = batch_threshold(I, skip_frac), ggm1 = I->ggm1;
+        const float tlo2 = skip_tlo2(batch_threshold(I, skip_frac)), ggm1 = I->ggm1;
         march3d<T>(S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy,
                    I->DtDz, [&](const Upd3<T> &o) {
                        if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
                        const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
-                       const float ub =
-                           speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1);
-                       if (!(ub < tlof)) acc.add_speed((double)speed3(o.r, o.u, o.v, o.w, o.E, ph));
+                       if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1, tlo2))
+                           acc.add_speed((double)speed3(o.r, o.u, o.v, o.w, o.E, ph));
                    });
         const int2 rg = ranges[it.x];
         if (publish_step<k3NT>(acc, parts, w, &I->done_items, rg.y, &s_last))
@@ -655,7 +654,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
         I.ph.divgamma = T(one / I.ph.gm1);
         I.ph.K = T(s.K);
         I.ph.kneg = I.ph.K < T(0);
-        I.ggm1 = (float)I.ph.gamma * (float)I.ph.gm1;
+        I.ggm1 = skip_ggm1(I.ph.gamma, I.ph.gm1);
         T first = 0;
         int rc;
         if constexpr (D == 2)

@@ -49,7 +49,7 @@ template <class T> struct Args2 {
     StepStatus *status;
     unsigned seq;
     unsigned long long key; // problem key for the signal-speed skip (0: never skip)
-    float ggm1;             // gamma * (gamma - 1), for the speed upper bound
+    float ggm1;             // gamma * (gamma - 1), for the signal-speed skip test
 };
 
 // The float skip threshold, rounded down so that every skipped cell is provably below
@@ -127,14 +127,14 @@ __global__ void __launch_bounds__(kStripNT, 4)
     const March2 geo{kStripW * (int)blockIdx.x, i0, min(i0 + g.chunk - 1, g.nb_x), g.nb_x, g.nb_y, g.ys};
     StepAcc acc;
     const float tlof = skip_threshold_f(g.scr, g.key);
-    const float ggm1 = g.ggm1;
+    const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
     const Phys<T> ph = g.ph;
     unsigned ld = 0;
     const bool ok = march2d<T>(S, &tmr, &tmu, geo, g.rhoE_n, g.uv_n, ph, g.DtDx, g.DtDy, ld, [&](const Upd2<T> &o) {
         acc.add_mass(o.r);
         const float fu = (float)o.u, fv = (float)o.v;
-        const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1);
-        if (!(ub < tlof)) acc.add_speed(speed2(o.r, o.u, o.v, o.E, ph));
+        if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1, tlo2))
+            acc.add_speed(speed2(o.r, o.u, o.v, o.E, ph));
     });
     if (!ok) acc.err |= kErrWaitTimeout;
     step_epilogue<kStripNT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y, blockIdx.x + blockIdx.y * gridDim.x,
@@ -282,7 +282,7 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
     g.nb_x = (int)nb_x; g.nb_y = (int)nb_y; g.ys = (long long)nb_y + 2;
     g.scr = ctx->scr; g.status = ctx->status_d; g.seq = ++ctx->seq;
     g.key = problem_key(Dt_next, nb_x, nb_y, 0, sizeof(T), ph);
-    g.ggm1 = (float)ph.gamma * (float)ph.gm1;
+    g.ggm1 = skip_ggm1(ph.gamma, ph.gm1);
 
     using V2 = typename Vec2<T>::type;
     const size_t rowbytes = 2 * sizeof(T) * (nb_y + 2);
@@ -567,7 +567,7 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
     g.nb_x = (int)NB_X; g.nb_y = (int)NB_Y; g.ys = (long long)NB_Y + 2;
     g.scr = scr; g.partials = partials; g.status = status; g.seq = 0;
     g.key = problem_key(Dt_next, NB_X, NB_Y, 0, sizeof(T), ph);
-    g.ggm1 = (float)gamma * (float)gamma_minus_one;
+    g.ggm1 = skip_ggm1(gamma, gamma_minus_one);
 
     const size_t rowbytes = 2 * sizeof(T) * (NB_Y + 2);
     bool strip_ok = aligned(d_rhoE, 16) && aligned(d_uv, 16) && aligned(d_rhoE_next, 16) && aligned(d_uv_next, 16) &&

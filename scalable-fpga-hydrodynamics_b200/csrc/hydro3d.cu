@@ -39,7 +39,7 @@ template <class T> struct Args3 {
     StepStatus *status;
     unsigned seq;
     unsigned long long key; // problem key for the signal-speed skip (0: never skip)
-    float ggm1;             // gamma * (gamma - 1), for the speed upper bound
+    float ggm1;             // gamma * (gamma - 1), for the signal-speed skip test
 };
 
 
@@ -114,13 +114,13 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
                      g.nb_x, g.nb_y, g.nb_z, g.zs, g.zy};
     StepAcc acc;
     const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
-    const float ggm1 = g.ggm1;
+    const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
     const Phys<T> ph = g.ph;
     march3d<T>(S, g.rhoE, g.uvw, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz, [&](const Upd3<T> &o) {
         acc.add_mass(o.r);
         const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
-        const float ub = speed_bound((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1);
-        if (!(ub < tlof)) acc.add_speed(speed3(o.r, o.u, o.v, o.w, o.E, ph));
+        if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1, tlo2))
+            acc.add_speed(speed3(o.r, o.u, o.v, o.w, o.E, ph));
     });
     step_epilogue<k3NT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
                            blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
@@ -213,7 +213,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
     g.zs = (long long)nb_z + 2; g.zy = (long long)(nb_y + 2) * g.zs;
     g.scr = ctx->scr; g.status = ctx->status_d; g.seq = ++ctx->seq;
     g.key = problem_key(Dt_next, nb_x, nb_y, nb_z, sizeof(T), ph);
-    g.ggm1 = (float)ph.gamma * (float)ph.gm1;
+    g.ggm1 = skip_ggm1(ph.gamma, ph.gm1);
 
     const bool use_strip = which != Kernel::Direct;
     unsigned nblocks;

@@ -201,34 +201,30 @@ template <class T> __device__ __forceinline__ T speed2(T r, T ru, T rv, T E, con
     return A::add(c_s, Unorm);
 }
 
-// A cheap upper bound of the signal speed, for skipping cells that cannot hold the
-// maximum. Since p = (gamma-1)(E - rho|u|^2/2) <= (gamma-1) E for E, rho > 0,
-//   c_s = sqrt(gamma p / rho) <= sqrt(gamma (gamma-1) E / rho),   |u| = |rho u| / rho.
-// Evaluated in FP32 with approximate reciprocal and square root (each within a few
-// units of 2^-23), then inflated by 2^-9, far above the accumulated rounding error.
-// Returns +inf when the inputs are outside the range where the FP32 evaluation is
-// safe, and NaN when E or rho is not positive (both send the cell to the exact path).
-__device__ __forceinline__ float rcp_approx(float x)
+// Whether the exact signal speed c_s + |u| of a new state is certainly below a threshold
+// tlo, for skipping cells that cannot hold the maximum. With m2 = |rho u|^2 and
+// ggm1 = gamma (gamma - 1): p = (gamma-1)(E - m2/(2 rho)) <= (gamma-1) E, so
+//   c_s^2 = gamma p / rho <= ggm1 E / rho,   |u|^2 = m2 / rho^2,
+// and with (a + b)^2 <= 2 (a^2 + b^2),
+//   (c_s + |u|)^2 <= 2 (ggm1 E rho + m2) / rho^2.
+// The speed is below tlo when 2 (ggm1 E rho + m2) < tlo^2 rho^2: no reciprocal and no
+// square root. Evaluated in FP32 for either precision of the state (FP64 kernels keep
+// their FP64 pipe for the update), with a relative margin of 2^-12, far above the
+// roundings of the conversions, of this test and of the exact speed's own evaluation, on
+// inputs in ranges where no product overflows or becomes subnormal; anything else (NaN,
+// non-positive rho or E, out of range) answers false and takes the exact path.
+__device__ __forceinline__ bool speed_below(float r, float E, float m2, float ggm1, float tlo2)
 {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
+    if (!(r > 1e-6f) || !(r < 1e6f) || !(E > 1e-6f) || !(E < 1e12f) || !(m2 < 1e24f)) return false;
+    return (ggm1 * E * r + m2) * (2.0f * (1.0f + 1.0f / 4096.0f)) < tlo2 * (r * r);
 }
-__device__ __forceinline__ float sqrt_approx(float x)
+// tlo^2 for speed_below; 0 (nothing skips) above the range the test is safe for
+__device__ __forceinline__ float skip_tlo2(float tlof) { return (tlof <= 1e6f) ? tlof * tlof : 0.0f; }
+// gamma (gamma - 1) in FP32 for speed_below; +inf (nothing skips) unless gamma > 1
+template <class T> __host__ __device__ inline float skip_ggm1(T gamma, T gm1)
 {
-    float y;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-__device__ __forceinline__ float speed_bound(float r, float E, float m2, float ggm1)
-{
-    // m2 = |rho u|^2 ; ggm1 = gamma * (gamma - 1)
-    if (!(r > 1e-18f) || !(r < 1e18f) || !(E > 1e-18f) || !(E < 1e18f) || !(m2 < 1e30f)) return __int_as_float(0x7f800000);
-    const float inv = rcp_approx(r);
-    const float c2 = ggm1 * E * inv;
-    const float u2 = m2 * inv * inv;
-    return (sqrt_approx(c2) + sqrt_approx(u2)) * 1.001953125f;
+    const float v = (float)gamma * (float)gm1;
+    return (gamma > T(1) && gm1 > T(0) && v > 0.0f) ? v : (float)(1.0 / 0.0);
 }
 
 // ---------------------------------------------------------------- 3D ----------------
