@@ -5,10 +5,12 @@
 // One block of 8 warps covers an 8 (y) x 32 (z) tile of columns starting at (jbase,
 // kbase): 6 x 30 interior columns plus a one-cell halo ring. Each lane copies its own
 // cell of each X plane into a k3Stages-deep shared-memory ring with cp.async (any
-// alignment of the interleaved pairs/triples), converts it to primitives once, and per
-// plane computes one x face (registers), one z face (warp shuffles) and one y face
-// (shared memory, double-buffered by plane parity; one barrier per plane), then updates
-// the plane behind it. Every updated interior cell is handed to `sink`.
+// alignment of the interleaved pairs/triples), converts it to primitives once and
+// publishes them as 16-byte pairs (double-buffered by plane parity; one barrier per
+// plane). Per plane a lane computes one x face (registers), one z face (the next lane's
+// cell from shared memory, the flux back by shuffles) and one y face (the warp above's
+// cell, the flux back through shared memory), then updates the plane behind it. Every
+// updated interior cell is handed to `sink`.
 #pragma once
 
 #include "hydro_rt.cuh"
@@ -40,11 +42,36 @@ template <int N> __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+template <class T> __device__ __forceinline__ typename Vec2<T>::type pair3(T a, T b)
+{
+    typename Vec2<T>::type v;
+    v.x = a;
+    v.y = b;
+    return v;
+}
+
 template <class T> struct Smem3 {
+    using V2 = typename Vec2<T>::type;
     T st[k3Stages][5][k3NT]; // per plane: rho, E, rho_u, rho_v, rho_w
-    T xP[2][9][k3NT];        // y-face inputs of each lane's cell, by plane parity
-    T xF[2][5][k3NT];        // each lane's +y face flux, by plane parity
+    // each lane's cell by plane parity, as pairs (r,p) (Ka,iKa) (v,w) (mu,mv) (mw,eup_xy)
+    // (eup_z,-): the warp below reads its y-face inputs, the previous lane its z-face inputs
+    V2 xP[2][6][k3NT];
+    V2 xF[2][2][k3NT]; // each lane's +y face flux by plane parity: (r,n) (t1,t2) ...
+    T xFE[2][k3NT];    // ... and E
 };
+
+// a neighbour's face inputs from the exchange buffer (layout of Smem3::xP)
+template <class T> __device__ __forceinline__ FaceIn3<T> xp_face_y(const typename Vec2<T>::type *x)
+{
+    const auto q0 = x[0 * k3NT], q1 = x[1 * k3NT], q2 = x[2 * k3NT], q3 = x[3 * k3NT], q4 = x[4 * k3NT];
+    return FaceIn3<T>{q0.x, q2.x, q0.y, q1.x, q1.y, q3.y, q3.x, q4.x, q4.y}; // normal v: (v, u, w)
+}
+template <class T> __device__ __forceinline__ FaceIn3<T> xp_face_z(const typename Vec2<T>::type *x)
+{
+    const auto q0 = x[0 * k3NT], q1 = x[1 * k3NT], q2 = x[2 * k3NT], q3 = x[3 * k3NT], q4 = x[4 * k3NT],
+               q5 = x[5 * k3NT];
+    return FaceIn3<T>{q0.x, q2.y, q0.y, q1.x, q1.y, q4.x, q3.y, q3.x, q5.x}; // normal w: (w, v, u)
+}
 
 struct March3 {
     int kbase, jbase, i0, i1; // tile corner (halo included) and interior X planes
@@ -107,11 +134,13 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
         }
         const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, ph);
         {
-            const FaceIn3<T> fy = face3_y(P);
-            T *x = &S.xP[m & 1][0][t];
-            x[0 * k3NT] = fy.r; x[1 * k3NT] = fy.un; x[2 * k3NT] = fy.p; x[3 * k3NT] = fy.Ka;
-            x[4 * k3NT] = fy.iKa; x[5 * k3NT] = fy.mn; x[6 * k3NT] = fy.mt1; x[7 * k3NT] = fy.mt2;
-            x[8 * k3NT] = fy.eup;
+            typename Smem3<T>::V2 *x = &S.xP[m & 1][0][t];
+            x[0 * k3NT] = pair3<T>(P.r, P.p);
+            x[1 * k3NT] = pair3<T>(P.Ka, P.iKa);
+            x[2 * k3NT] = pair3<T>(P.v, P.w);
+            x[3 * k3NT] = pair3<T>(P.mu, P.mv);
+            x[4 * k3NT] = pair3<T>(P.mw, P.eup_xy);
+            x[5 * k3NT] = pair3<T>(P.eup_z, T(0));
         }
         Flux3<T> fxhi{};
         if (m >= 1 && iwarp) fxhi = face_flux3(face3_x(Pm), face3_x(P), ph);
@@ -122,33 +151,23 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
             const FaceIn3<T> me = face3_y(Pm);
             Flux3<T> fy{};
             if (w < k3Warps - 1) {
-                const T *x = &S.xP[(m - 1) & 1][0][t + 32];
-                FaceIn3<T> nb{x[0 * k3NT], x[1 * k3NT], x[2 * k3NT], x[3 * k3NT], x[4 * k3NT],
-                              x[5 * k3NT], x[6 * k3NT], x[7 * k3NT], x[8 * k3NT]};
+                const FaceIn3<T> nb = xp_face_y<T>(&S.xP[(m - 1) & 1][0][t + 32]);
                 FaceIn3<T> L = me, R = nb;
                 if (kEdge) {
                     if (j == 0) L = mirror3(nb);
                     if (j == g.nb_y) R = mirror3(me);
                 }
                 fy = face_flux3(L, R, ph);
-                T *xf = &S.xF[m & 1][0][t];
-                xf[0 * k3NT] = fy.r; xf[1 * k3NT] = fy.n; xf[2 * k3NT] = fy.t1; xf[3 * k3NT] = fy.t2;
-                xf[4 * k3NT] = fy.E;
+                S.xF[m & 1][0][t] = pair3<T>(fy.r, fy.n);
+                S.xF[m & 1][1][t] = pair3<T>(fy.t1, fy.t2);
+                S.xFE[m & 1][t] = fy.E;
             }
-            // +z face of (k | k+1) via shuffles within the warp
+            // +z face of (k | k+1): the next lane's cell from the exchange buffer (lane 31
+            // reads the next warp's lane 0, a face no interior lane uses)
             Flux3<T> fz{};
             if (iwarp) {
                 const FaceIn3<T> mz = face3_z(Pm);
-                FaceIn3<T> nz;
-                nz.r = __shfl_down_sync(FULL, mz.r, 1);
-                nz.un = __shfl_down_sync(FULL, mz.un, 1);
-                nz.p = __shfl_down_sync(FULL, mz.p, 1);
-                nz.Ka = __shfl_down_sync(FULL, mz.Ka, 1);
-                nz.iKa = __shfl_down_sync(FULL, mz.iKa, 1);
-                nz.mn = __shfl_down_sync(FULL, mz.mn, 1);
-                nz.mt1 = __shfl_down_sync(FULL, mz.mt1, 1);
-                nz.mt2 = __shfl_down_sync(FULL, mz.mt2, 1);
-                nz.eup = __shfl_down_sync(FULL, mz.eup, 1);
+                const FaceIn3<T> nz = xp_face_z<T>(&S.xP[(m - 1) & 1][0][t + 1]);
                 FaceIn3<T> L = mz, R = nz;
                 if (kEdge) {
                     if (k == 0) L = mirror3(nz);
@@ -165,8 +184,8 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
                 fzl.t2 = __shfl_up_sync(FULL, fz.t2, 1);
                 fzl.E = __shfl_up_sync(FULL, fz.E, 1);
                 if (interior) {
-                    const T *xf = &S.xF[m & 1][0][t - 32];
-                    const Flux3<T> fyl{xf[0 * k3NT], xf[1 * k3NT], xf[2 * k3NT], xf[3 * k3NT], xf[4 * k3NT]};
+                    const auto a0 = S.xF[m & 1][0][t - 32], a1 = S.xF[m & 1][1][t - 32];
+                    const Flux3<T> fyl{a0.x, a0.y, a1.x, a1.y, S.xFE[m & 1][t - 32]};
                     const Upd3<T> o =
                         update3(Ur, Uu, Uv, Uw, UE, fxlo, fxhi, fyl, fy, fzl, fz, DtDx, DtDy, DtDz, ph);
                     const long long c = (long long)(g.i0 + m - 2) * g.zy + colofs;
