@@ -97,7 +97,10 @@ class queue {
         detail::check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
         q_.stream = s;
         q_.device = dev;
-        q_.flags = 0;
+        // HYDRO_B200_X_GHOSTS=memory: the kernels read the X ghost rows the host loop fills
+        // (a multi-rank --sdx run) instead of wrapping periodically in-kernel (one rank)
+        const char *xg = std::getenv("HYDRO_B200_X_GHOSTS");
+        q_.flags = (xg && std::strcmp(xg, "memory") == 0) ? HYDRO_X_GHOSTS_FROM_MEMORY : 0;
     }
     template <class S> explicit queue(const S &) : queue() {}
 

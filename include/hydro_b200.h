@@ -39,12 +39,21 @@ extern "C" {
 #endif
 
 /* The queue a launcher runs on: a CUDA stream (NULL = legacy default stream) and the
- * device it belongs to (-1 = the current device). */
+ * device it belongs to (-1 = the current device); flags: 0 or HYDRO_X_GHOSTS_FROM_MEMORY. */
 typedef struct hydro_queue {
     void *stream;
     int device;
     int flags;
 } hydro_queue_t;
+
+/* X boundary of a step. By default the kernels take the X neighbours of the first and
+ * last interior rows (planes) by periodic wrap inside the kernel: the whole domain is on
+ * one device and the input's X ghost rows are never read. With this bit set in
+ * hydro_queue_t.flags (launchers) or in the `kernel` argument (step entry points), they
+ * read the ghost rows 0 and NB_X+1 of the input instead, as the reference kernel does
+ * (hydro2d/kernel.cxx:152-170): the caller fills them, e.g. the reference's multi-rank
+ * host loop exchanging subdomain edges (hydro2d/main.cxx:349-424, --sdx N). */
+#define HYDRO_X_GHOSTS_FROM_MEMORY 0x100
 
 /* Extra results of one step, beyond what the reference's launcher returns. */
 typedef struct hydro_step_info {

@@ -24,6 +24,9 @@ LIB_DIR = PKG_DIR / "lib"
 LIB_PATH = LIB_DIR / "libhydro_b200.so"
 
 KERNEL_AUTO, KERNEL_STRIP, KERNEL_DIRECT = 0, 1, 2
+# X neighbours of the first and last interior rows (planes) from the input's ghost rows
+# instead of the in-kernel periodic wrap (include/hydro_b200.h)
+X_GHOSTS_FROM_MEMORY = 0x100
 HYDRO_OK, HYDRO_ERR_ARG, HYDRO_ERR_CUDA, HYDRO_ERR_NONPHYSICAL, HYDRO_ERR_TIMEOUT = 0, -1, -2, -3, -4
 
 _c_size = ctypes.c_size_t
@@ -208,9 +211,12 @@ def launcher3d(rhoE, uvw, rhoE_next, uvw_next, dt_next, C_min, gamma, gm1, divga
 
 
 def step(state_in, state_out, dt_next, phys: Physics, dtd, kernel=KERNEL_AUTO, sync=True, stream=None,
-         check=True):
-    """One step through hydro{2d,3d}_step_{f64,f32}. state_* = (rhoE, uvx) tensors."""
+         check=True, x_ghosts=False):
+    """One step through hydro{2d,3d}_step_{f64,f32}. state_* = (rhoE, uvx) tensors.
+    x_ghosts: read the X ghost rows (planes) of state_in instead of wrapping periodically."""
     L = lib()
+    if x_ghosts:
+        kernel |= X_GHOSTS_FROM_MEMORY
     f64 = phys.dtype is np.float64
     suf = "f64" if f64 else "f32"
     info = StepInfo()

@@ -78,7 +78,8 @@ double hydro2d_launcher_f64(const double *d_rhoE, const double *d_uv, double *d_
     }
     const int rc = step2d<double>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
                                   phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, *DtDx, *DtDy,
-                                  (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr);
+                                  (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr,
+                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
     return finish_launcher(rc, t0, "launcher");
 }
 
@@ -95,7 +96,8 @@ double hydro2d_launcher_f32(const float *d_rhoE, const float *d_uv, float *d_rho
     }
     const int rc = step2d<float>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, *DtDx, *DtDy,
-                                 (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr);
+                                 (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr,
+                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
     return finish_launcher(rc, t0, "launcher");
 }
 
@@ -113,7 +115,8 @@ double hydro3d_launcher_f64(const double *d_rhoE, const double *d_uvw, double *d
     }
     const int rc = step3d<double>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
                                   phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, *DtDx, *DtDy,
-                                  *DtDz, (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr);
+                                  *DtDz, (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr,
+                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
     return finish_launcher(rc, t0, "launcher");
 }
 
@@ -131,7 +134,8 @@ double hydro3d_launcher_f32(const float *d_rhoE, const float *d_uvw, float *d_rh
     }
     const int rc = step3d<float>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, *DtDx, *DtDy,
-                                 *DtDz, (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr);
+                                 *DtDz, (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr,
+                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
     return finish_launcher(rc, t0, "launcher");
 }
 
@@ -143,7 +147,8 @@ int hydro2d_step_f64(const double *d_rhoE, const double *d_uv, double *d_rhoE_ne
     StepInfo si;
     const int rc = step2d<double>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
                                   phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, DtDx, DtDy,
-                                  (cudaStream_t)stream, (Kernel)kernel, sync != 0, &si);
+                                  (cudaStream_t)stream, (Kernel)(kernel & 0xff), sync != 0, &si,
+                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
     fill(info, si);
     return rc;
 }
@@ -156,7 +161,8 @@ int hydro2d_step_f32(const float *d_rhoE, const float *d_uv, float *d_rhoE_next,
     StepInfo si;
     const int rc = step2d<float>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, DtDx, DtDy,
-                                 (cudaStream_t)stream, (Kernel)kernel, sync != 0, &si);
+                                 (cudaStream_t)stream, (Kernel)(kernel & 0xff), sync != 0, &si,
+                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
     fill(info, si);
     return rc;
 }
@@ -169,7 +175,8 @@ int hydro3d_step_f64(const double *d_rhoE, const double *d_uvw, double *d_rhoE_n
     StepInfo si;
     const int rc = step3d<double>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
                                   phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, DtDx, DtDy,
-                                  DtDz, (cudaStream_t)stream, (Kernel)kernel, sync != 0, &si);
+                                  DtDz, (cudaStream_t)stream, (Kernel)(kernel & 0xff), sync != 0, &si,
+                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
     fill(info, si);
     return rc;
 }
@@ -182,7 +189,8 @@ int hydro3d_step_f32(const float *d_rhoE, const float *d_uvw, float *d_rhoE_next
     StepInfo si;
     const int rc = step3d<float>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, DtDx, DtDy, DtDz,
-                                 (cudaStream_t)stream, (Kernel)kernel, sync != 0, &si);
+                                 (cudaStream_t)stream, (Kernel)(kernel & 0xff), sync != 0, &si,
+                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
     fill(info, si);
     return rc;
 }

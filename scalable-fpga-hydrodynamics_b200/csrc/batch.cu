@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(kStripNT, Batch2dOcc<T>::value) batch2d(Inst2<
         const int par = I->parity;
         const int strip = it.y % I->nstrips, ck = it.y / I->nstrips;
         const int i0 = 1 + ck * I->chunk;
-        const March2 geo{kStripW * strip, i0, min(i0 + I->chunk - 1, I->nb_x), I->nb_x, I->nb_y, I->ys};
+        const March2 geo{kStripW * strip, i0, min(i0 + I->chunk - 1, I->nb_x), I->nb_x, I->nb_y, I->ys, 1};
         const Phys<T> ph = I->ph;
         if (threadIdx.x == 0) {
             prefetch_tensormap(&I->tm[par][0]);
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *
         const int ty = rem % I->nty, ck = rem / I->nty;
         const int i0 = 1 + ck * I->chunk;
         const March3 geo{k3TZ * tz, k3TY * ty, i0, min(i0 + I->chunk - 1, I->nb_x), I->nb_x, I->nb_y, I->nb_z,
-                         I->zs, I->zy};
+                         I->zs, I->zy, 1};
         const Phys<T> ph = I->ph;
         MaxAcc acc;
         const float tlo2 = skip_tlo2(batch_threshold(I, skip_frac)), ggm1 = I->ggm1;

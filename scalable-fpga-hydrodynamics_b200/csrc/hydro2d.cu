@@ -50,6 +50,7 @@ template <class T> struct Args2 {
     unsigned seq;
     unsigned long long key; // problem key for the signal-speed skip (0: never skip)
     float ggm1;             // gamma * (gamma - 1), for the signal-speed skip test
+    int xwrap;              // X neighbours by periodic wrap (1) or from the ghost rows (0)
 };
 
 // The float skip threshold, rounded down so that every skipped cell is provably below
@@ -77,8 +78,8 @@ template <class T> __global__ void __launch_bounds__(kDirectNT) direct2d(Args2<T
         const long long c = (long long)i * g.ys + j;
         const T ur = g.rhoE[2 * c], uE = g.rhoE[2 * c + 1], uu = g.uv[2 * c], uv = g.uv[2 * c + 1];
         const Cell2<T> P = make_cell2<T>(ur, uu, uv, uE, g.ph);
-        const Cell2<T> PL = load_cell2(g, (long long)wrap_row(i - 1, g.nb_x) * g.ys + j);
-        const Cell2<T> PR = load_cell2(g, (long long)wrap_row(i + 1, g.nb_x) * g.ys + j);
+        const Cell2<T> PL = load_cell2(g, (long long)(g.xwrap ? wrap_row(i - 1, g.nb_x) : i - 1) * g.ys + j);
+        const Cell2<T> PR = load_cell2(g, (long long)(g.xwrap ? wrap_row(i + 1, g.nb_x) : i + 1) * g.ys + j);
         const Flux2<T> fx1 = face_flux(face_x(PL), face_x(P), g.ph);
         const Flux2<T> fx2 = face_flux(face_x(P), face_x(PR), g.ph);
         const FaceIn<T> me = face_y(P);
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(kStripNT, 4)
     }
     march2d_init(S);
     const int i0 = 1 + g.chunk * (int)blockIdx.y;
-    const March2 geo{kStripW * (int)blockIdx.x, i0, min(i0 + g.chunk - 1, g.nb_x), g.nb_x, g.nb_y, g.ys};
+    const March2 geo{kStripW * (int)blockIdx.x, i0, min(i0 + g.chunk - 1, g.nb_x), g.nb_x, g.nb_y, g.ys, g.xwrap};
     StepAcc acc;
     const float tlof = skip_threshold_f(g.scr, g.key);
     const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
@@ -246,7 +247,7 @@ bool aligned(const void *p, size_t a) { return (reinterpret_cast<uintptr_t>(p) %
 
 template <class T>
 int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
-           size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info)
+           size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info, bool xwrap)
 {
     if (!rhoE || !uv || !rhoE_next || !uv_next || !Dt_next) {
         set_error(kErrArg, "step2d: null pointer argument");
@@ -283,6 +284,7 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
     g.scr = ctx->scr; g.status = ctx->status_d; g.seq = ++ctx->seq;
     g.key = problem_key(Dt_next, nb_x, nb_y, 0, sizeof(T), ph);
     g.ggm1 = skip_ggm1(ph.gamma, ph.gm1);
+    g.xwrap = xwrap ? 1 : 0;
 
     using V2 = typename Vec2<T>::type;
     const size_t rowbytes = 2 * sizeof(T) * (nb_y + 2);
@@ -451,9 +453,9 @@ template <class T> int mass_sum(const T *rhoE, size_t nb_x, size_t nb_y, size_t 
 }
 
 template int step2d<double>(const double *, const double *, double *, double *, double *, const Phys<double> &,
-                            size_t, size_t, double, double, cudaStream_t, Kernel, bool, StepInfo *);
+                            size_t, size_t, double, double, cudaStream_t, Kernel, bool, StepInfo *, bool);
 template int step2d<float>(const float *, const float *, float *, float *, float *, const Phys<float> &, size_t,
-                           size_t, float, float, cudaStream_t, Kernel, bool, StepInfo *);
+                           size_t, float, float, cudaStream_t, Kernel, bool, StepInfo *, bool);
 template int init2d<double>(double *, double *, size_t, size_t, double, double, double, double, double, double,
                             double *, cudaStream_t);
 template int init2d_at<double>(double *, double *, size_t, size_t, double, double, double, double, double, double,
@@ -568,6 +570,7 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
     g.scr = scr; g.partials = partials; g.status = status; g.seq = 0;
     g.key = problem_key(Dt_next, NB_X, NB_Y, 0, sizeof(T), ph);
     g.ggm1 = skip_ggm1(gamma, gamma_minus_one);
+    g.xwrap = 1;
 
     const size_t rowbytes = 2 * sizeof(T) * (NB_Y + 2);
     bool strip_ok = aligned(d_rhoE, 16) && aligned(d_uv, 16) && aligned(d_rhoE_next, 16) && aligned(d_uv_next, 16) &&

@@ -40,6 +40,7 @@ template <class T> struct Args3 {
     unsigned seq;
     unsigned long long key; // problem key for the signal-speed skip (0: never skip)
     float ggm1;             // gamma * (gamma - 1), for the signal-speed skip test
+    int xwrap;              // X neighbours by periodic wrap (1) or from the ghost planes (0)
 };
 
 
@@ -60,8 +61,8 @@ template <class T> __global__ void __launch_bounds__(128) direct3d(Args3<T> g)
         const T ur = g.rhoE[2 * c], uE = g.rhoE[2 * c + 1];
         const T uu = g.uvw[3 * c], uv = g.uvw[3 * c + 1], uw = g.uvw[3 * c + 2];
         const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, g.ph);
-        const long long cxm = (long long)wrap_plane(i - 1, g.nb_x) * g.zy + (long long)j * g.zs + k;
-        const long long cxp = (long long)wrap_plane(i + 1, g.nb_x) * g.zy + (long long)j * g.zs + k;
+        const long long cxm = (long long)(g.xwrap ? wrap_plane(i - 1, g.nb_x) : i - 1) * g.zy + (long long)j * g.zs + k;
+        const long long cxp = (long long)(g.xwrap ? wrap_plane(i + 1, g.nb_x) : i + 1) * g.zy + (long long)j * g.zs + k;
         const Flux3<T> fx1 = face_flux3(face3_x(load_cell3(g, cxm)), face3_x(P), g.ph);
         const Flux3<T> fx2 = face_flux3(face3_x(P), face3_x(load_cell3(g, cxp)), g.ph);
         const FaceIn3<T> my = face3_y(P);
@@ -111,7 +112,7 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
     Smem3<T> &S = *reinterpret_cast<Smem3<T> *>(smem_raw);
     const int i0 = 1 + g.chunk * (int)blockIdx.z;
     const March3 geo{k3TZ * (int)blockIdx.x, k3TY * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
-                     g.nb_x, g.nb_y, g.nb_z, g.zs, g.zy};
+                     g.nb_x, g.nb_y, g.nb_z, g.zs, g.zy, g.xwrap};
     StepAcc acc;
     const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
     const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
@@ -177,7 +178,7 @@ __global__ void init3d_kernel(T *rhoE, T *uvw, int nb_x, int nb_y, int nb_z, lon
 template <class T>
 int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
            size_t nb_y, size_t nb_z, T DtDx, T DtDy, T DtDz, cudaStream_t stream, Kernel which, bool sync,
-           StepInfo *info)
+           StepInfo *info, bool xwrap)
 {
     if (!rhoE || !uvw || !rhoE_next || !uvw_next || !Dt_next) {
         set_error(kErrArg, "step3d: null pointer argument");
@@ -214,6 +215,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
     g.scr = ctx->scr; g.status = ctx->status_d; g.seq = ++ctx->seq;
     g.key = problem_key(Dt_next, nb_x, nb_y, nb_z, sizeof(T), ph);
     g.ggm1 = skip_ggm1(ph.gamma, ph.gm1);
+    g.xwrap = xwrap ? 1 : 0;
 
     const bool use_strip = which != Kernel::Direct;
     unsigned nblocks;
@@ -355,9 +357,10 @@ template int init3d_at<float>(float *, float *, size_t, size_t, size_t, double, 
                               float, float, float, float, float *, cudaStream_t, unsigned long long *);
 
 template int step3d<double>(const double *, const double *, double *, double *, double *, const Phys<double> &,
-                            size_t, size_t, size_t, double, double, double, cudaStream_t, Kernel, bool, StepInfo *);
+                            size_t, size_t, size_t, double, double, double, cudaStream_t, Kernel, bool, StepInfo *,
+                            bool);
 template int step3d<float>(const float *, const float *, float *, float *, float *, const Phys<float> &, size_t,
-                           size_t, size_t, float, float, float, cudaStream_t, Kernel, bool, StepInfo *);
+                           size_t, size_t, float, float, float, cudaStream_t, Kernel, bool, StepInfo *, bool);
 template int init3d<double>(double *, double *, size_t, size_t, size_t, double, double, double, double, double,
                             double, double *, cudaStream_t);
 template int init3d<float>(float *, float *, size_t, size_t, size_t, float, float, float, float, float, float,

@@ -105,15 +105,19 @@ struct StepInfo {
 };
 
 // One FVM step on the whole domain (periodic X by in-kernel wrap, reflective Y[/Z]).
-// Launches on `stream`, and when `sync` is true waits for it and fills *info.
+// Launches on `stream`, and when `sync` is true waits for it and fills *info. xwrap:
+// X neighbours of the first and last interior rows (planes) by periodic wrap inside the
+// kernel (the whole domain on one device); false: from the ghost rows 0 and NB_X+1 of the
+// input, filled by the caller (a subdomain of a multi-rank run).
 template <class T>
 int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
-           size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info);
+           size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info,
+           bool xwrap = true);
 
 template <class T>
 int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
            size_t nb_y, size_t nb_z, T DtDx, T DtDy, T DtDz, cudaStream_t stream, Kernel which, bool sync,
-           StepInfo *info);
+           StepInfo *info, bool xwrap = true);
 
 // Blast initial condition and first Dt on the device (hydro2d/main.cxx:280-338).
 template <class T>

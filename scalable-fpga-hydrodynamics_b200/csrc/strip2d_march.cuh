@@ -56,6 +56,7 @@ struct March2 {
     int jbase, i0, i1; // columns jbase .. jbase+kStripNT-1, interior rows i0 .. i1
     int nb_x, nb_y;
     long long ys;
+    int xwrap; // X neighbours of rows 1 and NB_X by periodic wrap (1) or ghost rows (0)
 };
 
 // kEdge = false: a strip whose every lane holds a real column (1 <= j <= NB_Y), so no
@@ -85,7 +86,7 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
     auto issue = [&](int m) {
         const unsigned q = ld0 + (unsigned)m;
         const int s = q % kStages;
-        const int row = wrap_row(g.i0 - 1 + m, g.nb_x);
+        const int row = g.xwrap ? wrap_row(g.i0 - 1 + m, g.nb_x) : g.i0 - 1 + m;
         mbar_arrive_expect_tx(&S.full[s], kStageBytes);
         tma_load_2d(&S.sr[s][0], tmr, xcoord, row, &S.full[s]);
         tma_load_2d(&S.su[s][0], tmu, xcoord, row, &S.full[s]);

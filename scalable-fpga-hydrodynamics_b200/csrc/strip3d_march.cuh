@@ -77,6 +77,7 @@ struct March3 {
     int kbase, jbase, i0, i1; // tile corner (halo included) and interior X planes
     int nb_x, nb_y, nb_z;
     long long zs, zy; // strides in cells of a Y row and of an X plane
+    int xwrap;        // X neighbours of planes 1 and NB_X by periodic wrap (1) or ghost planes (0)
 };
 
 // kEdge = false: a tile whose every lane holds a real cell (1 <= j <= NB_Y,
@@ -103,7 +104,7 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
     auto issue = [&](int m) {
         const int s = m % k3Stages;
         if (m < nplanes) {
-            const long long c = (long long)wrap_plane(g.i0 - 1 + m, g.nb_x) * g.zy + colofs;
+            const long long c = (long long)(g.xwrap ? wrap_plane(g.i0 - 1 + m, g.nb_x) : g.i0 - 1 + m) * g.zy + colofs;
             const T *pr = in_array ? rhoE + 2 * c : rhoE;
             const T *pu = in_array ? uvw + 3 * c : uvw;
             cp_async(&S.st[s][0][t], pr, sizeof(T), in_array);

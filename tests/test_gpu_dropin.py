@@ -5,6 +5,7 @@ target `dropin`) against the same program with the reference kernel on the CPU
 output files on the small configurations."""
 from __future__ import annotations
 
+import os
 import re
 import subprocess
 from pathlib import Path
@@ -25,8 +26,9 @@ CASES = [
 ]
 
 
-def run(exe: Path, args, cwd: Path, with_mass: bool):
-    p = subprocess.run([str(exe)] + args, cwd=cwd, capture_output=True, text=True, timeout=600)
+def run(exe: Path, args, cwd: Path, with_mass: bool, env=None):
+    p = subprocess.run([str(exe)] + args, cwd=cwd, capture_output=True, text=True, timeout=600,
+                       env=None if env is None else {**os.environ, **env})
     assert p.returncode == 0, p.stderr[-2000:]
     lines = []
     for line in p.stdout.splitlines():
@@ -39,8 +41,19 @@ def run(exe: Path, args, cwd: Path, with_mass: bool):
     return lines
 
 
-@pytest.mark.parametrize("prog,args", CASES)
-def test_dropin_main_matches_reference_program(prog, args, tmp_path):
+# X slabs (--sdx N --sdy 1): the host program exchanges the subdomains' edge rows itself;
+# the kernels read them from the X ghost rows (HYDRO_B200_X_GHOSTS=memory)
+SLAB_CASES = [
+    ("hydro", ["-x", "60", "-y", "60", "-t", "2", "-i", "120", "-w", "40", "--sdx", "2", "--sdy", "1"]),
+    ("hydro", ["-x", "48", "-y", "30", "-t", "2", "-i", "80", "-w", "40", "--sdx", "3", "--sdy", "1"]),
+    ("hydro_float", ["-x", "60", "-y", "60", "-t", "2", "-i", "120", "-w", "40", "--sdx", "2", "--sdy", "1"]),
+    ("hydro3d", ["-x", "20", "-y", "16", "-z", "12", "-t", "2", "-i", "40", "-w", "20", "--sdx", "2", "--sdy", "1"]),
+]
+
+
+@pytest.mark.parametrize("prog,args,env", [(p, a, None) for p, a in CASES] +
+                         [(p, a, {"HYDRO_B200_X_GHOSTS": "memory"}) for p, a in SLAB_CASES])
+def test_dropin_main_matches_reference_program(prog, args, env, tmp_path):
     gpu, cpu = REFDIR / f"{prog}.cuda", REFDIR / f"{prog}.cpu"
     if not gpu.exists() or not cpu.exists():
         pytest.skip("oracle/_ref drop-in binaries not built")
@@ -50,7 +63,7 @@ def test_dropin_main_matches_reference_program(prog, args, tmp_path):
     # the printed value uninitialised (hydro2d/main.cxx:261-263): mass lines are compared
     # for the FP64 programs only
     with_mass = not prog.endswith("_float")
-    out_gpu = run(gpu, args, tmp_path / "gpu", with_mass)
+    out_gpu = run(gpu, args, tmp_path / "gpu", with_mass, env)
     out_cpu = run(cpu, args, tmp_path / "cpu", with_mass)
     assert out_gpu == out_cpu
     files = sorted(p.name for p in (tmp_path / "cpu").glob("*.csv"))

@@ -241,3 +241,34 @@ def test_empty_grid(cuda):
     dt = cuda.zeros(1, dtype=cuda.float64, device="cuda")
     hb.step(cur, nxt, dt, phys, phys.dtd(np.float64(1e-3)))
     assert dt.item() == float("inf")
+
+
+@pytest.mark.parametrize("kernel", [hb.KERNEL_STRIP, hb.KERNEL_DIRECT])
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+@pytest.mark.parametrize("nb", [(7, 130), (33, 18), (3, 2, 33), (9, 14, 61)])
+def test_step_x_ghosts_from_memory(cuda, oracle, nb, T, kernel):
+    """With X_GHOSTS_FROM_MEMORY the kernels read the X ghost rows (planes) the caller
+    filled, as the reference kernel does: arbitrary (non-periodic) ghost contents, bit for
+    bit against the oracle, which reads them too."""
+    phys = hb.Physics(T, nb)
+    for seed in range(2):
+        st = seeded_state(nb, T, seed)
+        other = seeded_state(nb, T, seed + 10)  # ghost rows taken from an unrelated state
+        row = int(np.prod([n + 2 for n in nb[1:]]))
+        for a, b, nv in zip(st, other, (2, len(nb))):
+            k = row * nv
+            a[:k] = b[k:2 * k]
+            a[-k:] = b[-2 * k:-k]
+        ref = (np.zeros_like(st[0]), np.zeros_like(st[1]))
+        dtd = phys.dtd(cfl_dt(phys, seed))
+        dref = oracle.step(st, ref, phys, dtd)
+        cur = to_dev(cuda, st)
+        nxt = tuple(cuda.zeros_like(a) for a in cur)
+        dt = cuda.zeros(1, dtype=cur[0].dtype, device="cuda")
+        if kernel == hb.KERNEL_STRIP and len(nb) == 2 and T is np.float32 and (nb[1] + 2) % 2:
+            continue
+        _, info = hb.step(cur, nxt, dt, phys, dtd, kernel=kernel, x_ghosts=True)
+        assert info.kernel == kernel
+        assert phys.dtype(dt.item()).tobytes() == dref.tobytes()
+        out = tuple(a.cpu().numpy() for a in nxt)
+        assert out[0].tobytes() == ref[0].tobytes() and out[1].tobytes() == ref[1].tobytes()

@@ -130,3 +130,17 @@ def test_replicas_single_process_is_identity():
     assert r.max_over_ranks(3.5) == 3.5 and r.share([1, 2, 3]) == [1, 2, 3]
     r.barrier()
     r.close()
+
+
+def test_slab_rows_partition():
+    from hydro_b200.slabs import slab_rows
+
+    for nb_x in (1, 7, 40000):
+        for world in range(1, min(nb_x, 9) + 1):
+            rows = [slab_rows(nb_x, world, r) for r in range(world)]
+            assert rows[0][0] == 1 and rows[-1][1] == nb_x
+            assert all(b[0] == a[1] + 1 for a, b in zip(rows, rows[1:]))
+            sizes = [hi - lo + 1 for lo, hi in rows]
+            assert max(sizes) - min(sizes) <= 1 and min(sizes) >= 1
+    with pytest.raises(hb.HydroError):
+        slab_rows(2, 3, 0)
