@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(kStripNT, Batch2dOcc<T>::value) batch2d(Inst2<
 }
 
 template <class T>
-__global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *items, const int2 *ranges,
+__global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) batch3d(Inst3<T> *insts, const int2 *items, const int2 *ranges,
                                                   int nitems, unsigned *counter, ItemPart *parts,
                                                   SlotStatus *status, double skip_frac)
 {
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *
         const int tz = it.y % I->ntz, rem = it.y / I->ntz;
         const int ty = rem % I->nty, ck = rem / I->nty;
         const int i0 = 1 + ck * I->chunk;
-        const March3 geo{k3TZ * tz, k3TY * ty, i0, min(i0 + I->chunk - 1, I->nb_x), I->nb_x, I->nb_y, I->nb_z,
+        const March3 geo{k3TZ * tz, k3TY<T> * ty, i0, min(i0 + I->chunk - 1, I->nb_x), I->nb_x, I->nb_y, I->nb_z,
                          I->zs, I->zy, 1};
         const Phys<T> ph = I->ph;
         MaxAcc acc;
@@ -452,8 +452,8 @@ __global__ void __launch_bounds__(k3NT, 2) batch3d(Inst3<T> *insts, const int2 *
                            acc.add_speed((double)speed3(o.r, o.u, o.v, o.w, o.E, ph));
                    });
         const int2 rg = ranges[it.x];
-        if (publish_step<k3NT>(acc, parts, w, &I->done_items, rg.y, &s_last))
-            finalize_step<k3NT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
+        if (publish_step<k3NT<T>>(acc, parts, w, &I->done_items, rg.y, &s_last))
+            finalize_step<k3NT<T>, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
     }
 }
 
@@ -479,8 +479,8 @@ template <int NT, class T> __device__ __forceinline__ void sum_item(const Inst3<
     const int tz = y % I->ntz, rem = y / I->ntz;
     const int ty = rem % I->nty, ck = rem / I->nty;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int k = k3TZ * tz + lane, j = k3TY * ty + w;
-    if (w < 1 || w > k3TY || lane < 1 || lane > k3TZ || j > I->nb_y || k > I->nb_z) return;
+    const int k = k3TZ * tz + lane, j = k3TY<T> * ty + w;
+    if (w < 1 || w > k3TY<T> || lane < 1 || lane > k3TZ || j > I->nb_y || k > I->nb_z) return;
     const int i0 = 1 + ck * I->chunk, i1 = min(i0 + I->chunk - 1, I->nb_x);
     const T *r = I->rhoE[I->parity], *u = I->uvw[I->parity];
     for (int i = i0; i <= i1; ++i) {
@@ -555,7 +555,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
             smem_ = (int)sizeof(Smem3<T>);
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(batch3d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_);
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch3d<T>, k3NT, smem_);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch3d<T>, k3NT<T>, smem_);
         }
         blocks_ = nsm * std::max(1, occ);
         int occ_s = 0;
@@ -563,7 +563,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
             if constexpr (D == 2)
                 e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, batch_sums<kStripNT, T, Inst>, kStripNT, 0);
             else
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, batch_sums<k3NT, T, Inst>, k3NT, 0);
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, batch_sums<k3NT<T>, T, Inst>, k3NT<T>, 0);
         }
         sum_blocks_ = nsm * std::max(1, occ_s);
         slots_.resize(cap_);
@@ -706,7 +706,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
             I.zs = (long long)nb_z + 2;
             I.zy = (long long)(nb_y + 2) * I.zs;
             I.ntz = (int)((nb_z + k3TZ - 1) / k3TZ);
-            I.nty = (int)((nb_y + k3TY - 1) / k3TY);
+            I.nty = (int)((nb_y + k3TY<T> - 1) / k3TY<T>);
             for (int b = 0; b < 2; ++b) {
                 I.rhoE[b] = sl.rhoE[b];
                 I.uvw[b] = sl.uvx[b];
@@ -886,7 +886,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
             batch2d<T><<<blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
                                                          status_d_, skip_frac_);
         else
-            batch3d<T><<<blocks_, k3NT, smem_, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
+            batch3d<T><<<blocks_, k3NT<T>, smem_, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
                                                          status_d_, skip_frac_);
     }
 
@@ -896,7 +896,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
             batch_sums<kStripNT, T, Inst><<<sum_blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_,
                                                                                 counter_ + 1, parts_, status_d_);
         else
-            batch_sums<k3NT, T, Inst><<<sum_blocks_, k3NT, 0, stream_>>>(insts_, items_, ranges_, nitems_,
+            batch_sums<k3NT<T>, T, Inst><<<sum_blocks_, k3NT<T>, 0, stream_>>>(insts_, items_, ranges_, nitems_,
                                                                         counter_ + 1, parts_, status_d_);
     }
 

@@ -106,12 +106,12 @@ template <class T> __global__ void __launch_bounds__(k3RedoNT) redo3d(Args3<T> g
 }
 
 // ------------------------------------------------------------------- strip kernel ---
-template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g)
+template <class T> __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) strip3d(Args3<T> g)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem3<T> &S = *reinterpret_cast<Smem3<T> *>(smem_raw);
     const int i0 = 1 + g.chunk * (int)blockIdx.z;
-    const March3 geo{k3TZ * (int)blockIdx.x, k3TY * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
+    const March3 geo{k3TZ * (int)blockIdx.x, k3TY<T> * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
                      g.nb_x, g.nb_y, g.nb_z, g.zs, g.zy, g.xwrap};
     StepAcc acc;
     const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
@@ -123,7 +123,7 @@ template <class T> __global__ void __launch_bounds__(k3NT, 2) strip3d(Args3<T> g
         if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1, tlo2))
             acc.add_speed(speed3(o.r, o.u, o.v, o.w, o.E, ph));
     });
-    step_epilogue<k3NT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
+    step_epilogue<k3NT<T>, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
                            blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
                            g.status, g.seq, (double)tlof, g.key);
 }
@@ -220,7 +220,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
     const bool use_strip = which != Kernel::Direct;
     unsigned nblocks;
     if (use_strip) {
-        const int nz = (int)((nb_z + k3TZ - 1) / k3TZ), ny = (int)((nb_y + k3TY - 1) / k3TY);
+        const int nz = (int)((nb_z + k3TZ - 1) / k3TZ), ny = (int)((nb_y + k3TY<T> - 1) / k3TY<T>);
         if (ny > 65535) {
             set_error(kErrArg, "step3d: NB_Y %zu too large for the strip kernel", nb_y);
             return kErrArg;
@@ -244,7 +244,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
             set_error(kErrCuda, "step3d: shared-memory attribute: %s", cudaGetErrorString(ea));
             return kErrCuda;
         }
-        strip3d<T><<<dim3(nz, ny, nchunks), k3NT, smem, stream>>>(g);
+        strip3d<T><<<dim3(nz, ny, nchunks), k3NT<T>, smem, stream>>>(g);
     } else {
         const int gx = (int)((nb_z + 31) / 32), gy = (int)((nb_y + 3) / 4), gz = (int)std::min<size_t>(nb_x, 65535);
         if (gy > 65535) {

@@ -17,9 +17,14 @@
 
 namespace hydro {
 
-constexpr int k3Warps = 8;         // y extent of the tile (with halo)
-constexpr int k3NT = 32 * k3Warps; // threads
-constexpr int k3TY = k3Warps - 2;  // interior rows per tile
+// Tile height per precision: FP32 keeps 16 warps (14 interior rows; one 512-thread block
+// per SM), FP64 8 warps (6 interior rows; two 256-thread blocks per SM, the most its
+// 128-register budget allows). Measured at 512^3: FP32 48.3 -> 50.1 GCell/s with 16 warps,
+// FP64 31.5 -> 28.4 (it spills and loses the second block).
+template <class T> constexpr int k3Warps = sizeof(T) == 4 ? 16 : 8; // y extent of the tile (with halo)
+template <class T> constexpr int k3NT = 32 * k3Warps<T>;             // threads
+template <class T> constexpr int k3TY = k3Warps<T> - 2;              // interior rows per tile
+template <class T> constexpr int k3MinBlocks = k3Warps<T> <= 8 ? 2 : 1; // resident blocks per SM
 constexpr int k3TZ = 30;           // interior columns per tile
 constexpr int k3Stages = 4;
 
@@ -52,24 +57,24 @@ template <class T> __device__ __forceinline__ typename Vec2<T>::type pair3(T a, 
 
 template <class T> struct Smem3 {
     using V2 = typename Vec2<T>::type;
-    T st[k3Stages][5][k3NT]; // per plane: rho, E, rho_u, rho_v, rho_w
+    T st[k3Stages][5][k3NT<T>]; // per plane: rho, E, rho_u, rho_v, rho_w
     // each lane's cell by plane parity, as pairs (r,p) (Ka,iKa) (v,w) (mu,mv) (mw,eup_xy)
     // (eup_z,-): the warp below reads its y-face inputs, the previous lane its z-face inputs
-    V2 xP[2][6][k3NT];
-    V2 xF[2][2][k3NT]; // each lane's +y face flux by plane parity: (r,n) (t1,t2) ...
-    T xFE[2][k3NT];    // ... and E
+    V2 xP[2][6][k3NT<T>];
+    V2 xF[2][2][k3NT<T>]; // each lane's +y face flux by plane parity: (r,n) (t1,t2) ...
+    T xFE[2][k3NT<T>];    // ... and E
 };
 
 // a neighbour's face inputs from the exchange buffer (layout of Smem3::xP)
 template <class T> __device__ __forceinline__ FaceIn3<T> xp_face_y(const typename Vec2<T>::type *x)
 {
-    const auto q0 = x[0 * k3NT], q1 = x[1 * k3NT], q2 = x[2 * k3NT], q3 = x[3 * k3NT], q4 = x[4 * k3NT];
+    const auto q0 = x[0 * k3NT<T>], q1 = x[1 * k3NT<T>], q2 = x[2 * k3NT<T>], q3 = x[3 * k3NT<T>], q4 = x[4 * k3NT<T>];
     return FaceIn3<T>{q0.x, q2.x, q0.y, q1.x, q1.y, q3.y, q3.x, q4.x, q4.y}; // normal v: (v, u, w)
 }
 template <class T> __device__ __forceinline__ FaceIn3<T> xp_face_z(const typename Vec2<T>::type *x)
 {
-    const auto q0 = x[0 * k3NT], q1 = x[1 * k3NT], q2 = x[2 * k3NT], q3 = x[3 * k3NT], q4 = x[4 * k3NT],
-               q5 = x[5 * k3NT];
+    const auto q0 = x[0 * k3NT<T>], q1 = x[1 * k3NT<T>], q2 = x[2 * k3NT<T>], q3 = x[3 * k3NT<T>], q4 = x[4 * k3NT<T>],
+               q5 = x[5 * k3NT<T>];
     return FaceIn3<T>{q0.x, q2.y, q0.y, q1.x, q1.y, q4.x, q3.y, q3.x, q5.x}; // normal w: (w, v, u)
 }
 
@@ -93,8 +98,8 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
     const int nplanes = g.i1 - g.i0 + 3;
     const bool in_array = !kEdge || ((j <= g.nb_y + 1) && (k <= g.nb_z + 1));
     const bool interior =
-        (w >= 1) && (w <= k3TY) && (lane >= 1) && (lane <= k3TZ) && (!kEdge || ((j <= g.nb_y) && (k <= g.nb_z)));
-    const bool iwarp = (w >= 1) && (w <= k3TY) && (!kEdge || (g.jbase + 1 <= g.nb_y)); // warp holds interior rows
+        (w >= 1) && (w <= k3TY<T>) && (lane >= 1) && (lane <= k3TZ) && (!kEdge || ((j <= g.nb_y) && (k <= g.nb_z)));
+    const bool iwarp = (w >= 1) && (w <= k3TY<T>) && (!kEdge || (g.jbase + 1 <= g.nb_y)); // warp holds interior rows
     const long long colofs = (long long)j * g.zs + k;
     // ghost cells (j or k = 0 or NB+1) and cells past the array are never used: they
     // convert a unit state so every lane's reciprocal / square root stays regular
@@ -136,12 +141,12 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
         const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, ph);
         {
             typename Smem3<T>::V2 *x = &S.xP[m & 1][0][t];
-            x[0 * k3NT] = pair3<T>(P.r, P.p);
-            x[1 * k3NT] = pair3<T>(P.Ka, P.iKa);
-            x[2 * k3NT] = pair3<T>(P.v, P.w);
-            x[3 * k3NT] = pair3<T>(P.mu, P.mv);
-            x[4 * k3NT] = pair3<T>(P.mw, P.eup_xy);
-            x[5 * k3NT] = pair3<T>(P.eup_z, T(0));
+            x[0 * k3NT<T>] = pair3<T>(P.r, P.p);
+            x[1 * k3NT<T>] = pair3<T>(P.Ka, P.iKa);
+            x[2 * k3NT<T>] = pair3<T>(P.v, P.w);
+            x[3 * k3NT<T>] = pair3<T>(P.mu, P.mv);
+            x[4 * k3NT<T>] = pair3<T>(P.mw, P.eup_xy);
+            x[5 * k3NT<T>] = pair3<T>(P.eup_z, T(0));
         }
         Flux3<T> fxhi{};
         if (m >= 1 && iwarp) fxhi = face_flux3(face3_x(Pm), face3_x(P), ph);
@@ -151,7 +156,7 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
             // +y face of (j | j+1), from this lane's previous-plane cell and the warp above's
             const FaceIn3<T> me = face3_y(Pm);
             Flux3<T> fy{};
-            if (w < k3Warps - 1) {
+            if (w < k3Warps<T> - 1) {
                 const FaceIn3<T> nb = xp_face_y<T>(&S.xP[(m - 1) & 1][0][t + 32]);
                 FaceIn3<T> L = me, R = nb;
                 if (kEdge) {
@@ -215,7 +220,7 @@ __device__ __forceinline__ void march3d(Smem3<T> &S, const T *rhoE, const T *uvw
                                         const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &&sink)
 {
     const bool inner =
-        g.jbase >= 1 && g.jbase + k3Warps - 1 <= g.nb_y && g.kbase >= 1 && g.kbase + 31 <= g.nb_z;
+        g.jbase >= 1 && g.jbase + k3Warps<T> - 1 <= g.nb_y && g.kbase >= 1 && g.kbase + 31 <= g.nb_z;
     if (inner)
         march3d_tile<false>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
     else
