@@ -100,6 +100,24 @@ double hydro3d_launcher_f32(const float *d_rhoE, const float *d_uvw, float *d_rh
                             size_t NB_X, size_t NB_Y, size_t NB_Z, const float *DtDx, const float *DtDy,
                             const float *DtDz, hydro_queue_t queue);
 
+/* ---- CSV output formatted on the GPU --------------------------------------------- */
+/* Write a state (device arrays, reference layout) as the reference's write_results does
+ * (hydro2d/main.cxx:166-235, hydro3d/main.cxx:172-247): the header "x,y,rho,p,u,v"
+ * ("x,y,z,rho,p,u,v,w"), then one line "i,j[,k],rho,E,rho_u,rho_v[,rho_w]" per interior
+ * cell in row-major order, i = i_offset + row - 1, each value as std::ostream writes it
+ * (printf %g: 6 significant digits, correctly rounded). Byte-identical to the reference's
+ * files. Returns the bytes written, or a negative error code. */
+long long hydro2d_write_csv_f64(const double *d_rhoE, const double *d_uv, size_t NB_X, size_t NB_Y, size_t i_offset,
+                                const char *path, void *stream);
+long long hydro2d_write_csv_f32(const float *d_rhoE, const float *d_uv, size_t NB_X, size_t NB_Y, size_t i_offset,
+                                const char *path, void *stream);
+long long hydro3d_write_csv_f64(const double *d_rhoE, const double *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z,
+                                size_t i_offset, const char *path, void *stream);
+long long hydro3d_write_csv_f32(const float *d_rhoE, const float *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z,
+                                size_t i_offset, const char *path, void *stream);
+/* printf("%g") of n device doubles into d_out, 16 NUL-padded bytes per value. */
+int hydro_format_g(const double *d_values, size_t n, char *d_out, void *stream);
+
 /* ---- step entry points with explicit stream, kernel choice and results ------------ */
 /* Same arithmetic as the launchers (hydro2d/kernel.cxx:132-319, hydro3d/kernel.cxx:
  * 145-407) with DtDx.. by value. sync = 0 only enqueues on `stream` (info->kernel is

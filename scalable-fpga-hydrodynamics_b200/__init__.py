@@ -285,6 +285,35 @@ def mass(rhoE, nb, stream=None) -> float:
     return out.value
 
 
+def write_csv(state, nb, path, i_offset=0, stream=None) -> int:
+    """The state (reference layout, device tensors) as the reference's CSV output file,
+    formatted on the GPU (hydro{2d,3d}_write_csv_*); returns the bytes written."""
+    L = lib()
+    f64 = state[0].dtype.itemsize == 8
+    suf = "f64" if f64 else "f32"
+    fn = getattr(L, f"hydro{len(nb)}d_write_csv_{suf}")
+    fn.argtypes = [_vp, _vp] + [_c_size] * (len(nb) + 1) + [ctypes.c_char_p, _vp]
+    fn.restype = ctypes.c_longlong
+    n = fn(_ptr(state[0]), _ptr(state[1]), *[int(x) for x in nb], int(i_offset), str(path).encode(),
+           _stream_handle(stream))
+    if n < 0:
+        raise HydroError(int(n), last_error()[1])
+    return int(n)
+
+
+def format_g(values) -> list:
+    """printf("%g") of each double, formatted on the GPU (hydro_format_g)."""
+    torch = _torch()
+    v = torch.as_tensor(np.ascontiguousarray(values, dtype=np.float64)).cuda()
+    out = torch.zeros(max(1, v.numel()) * 16, dtype=torch.uint8, device="cuda")
+    L = lib()
+    L.hydro_format_g.argtypes = [_vp, _c_size, _vp, _vp]
+    L.hydro_format_g.restype = ctypes.c_int
+    _check(L.hydro_format_g(_ptr(v), v.numel(), _ptr(out), None))
+    raw = out.cpu().numpy().reshape(-1, 16)[:v.numel()]
+    return [bytes(r).split(b"\0", 1)[0].decode() for r in raw]
+
+
 def alloc_state(nb, dtype, device="cuda"):
     """(rhoE, uv[w]) device arrays of the reference layout, zero-initialised."""
     torch = _torch()
