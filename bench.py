@@ -552,7 +552,10 @@ def main():
         for name, vnb, T in (("2d_f32_40000x20000", nb, np.float32), ("3d_f64_512^3", (512, 512, 512), np.float64),
                              ("3d_f32_512^3", (512, 512, 512), np.float32)):
             barrier()
+            vsampler = ClockSampler(uuid)
+            vsampler.start()
             vr = bench_resident(hb, torch, vnb, T, max(5, args.steps // 3), 3)
+            vclocks = vsampler.stop()
             barrier()
             vms = max_over_ranks(vr["total_ms"])
             nst = max(5, args.steps // 3)
@@ -561,7 +564,7 @@ def main():
             bpc = BYTES_PER_CELL[(len(vnb), np.dtype(T).itemsize)]
             variants[name] = dict(value=world * vc * nst / (vms / 1e3) / 1e9, unit=UNIT,
                                   kernel_gbs=vc * bpc / (km / 1e3) / 1e9, frac=vc * bpc / (km / 1e3) / 1e9 / hbm,
-                                  kernel=int(vr["kernel"]), ms_per_step=vms / nst)
+                                  kernel=int(vr["kernel"]), ms_per_step=vms / nst, clocks=vclocks)
 
     log = lambda msg: print(msg, file=sys.stderr, flush=True)
     batched = serving = None
