@@ -83,6 +83,7 @@ struct SlotStatus {
     unsigned err;
 };
 
+// The end-of-run conservation sums of one item (compensated FP64), merged per instance.
 struct BatchAcc {
     double s[kSums] = {0, 0, 0, 0, 0}, c[kSums] = {0, 0, 0, 0, 0};
     double vmax = 0.0;
@@ -104,11 +105,6 @@ struct BatchAcc {
         if (D == 3) kahan(3, (double)mw);
         kahan(4, (double)E);
         if (!(r > T(0))) err |= kErrNonPhysical;
-    }
-    __device__ __forceinline__ void add_speed(double sp)
-    {
-        vmax = (sp > vmax) ? sp : vmax;
-        if (!(sp <= 1.0e300)) err |= kErrNonPhysical;
     }
 };
 
