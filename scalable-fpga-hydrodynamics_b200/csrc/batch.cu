@@ -367,7 +367,7 @@ __device__ __forceinline__ bool publish_item(BatchAcc &acc, ItemPart *parts, int
 }
 
 // resident blocks per SM the register budget of the 2D step aims at
-template <class T> struct Batch2dOcc { static constexpr int value = sizeof(T) == 4 ? 5 : 4; };
+template <class T> struct Batch2dOcc { static constexpr int value = sizeof(T) == 4 ? 6 : 4; };
 
 template <class T>
 __global__ void __launch_bounds__(kStripNT, Batch2dOcc<T>::value) batch2d(Inst2<T> *insts, const int2 *items, const int2 *ranges,
