@@ -22,6 +22,7 @@
 #include <math.h>
 #include <mutex>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include "../../include/hydro_b200.h"
 #include "hydro_host.h"
@@ -333,7 +334,12 @@ long long write_csv(const T *rhoE, const T *uvx, size_t nb_x, size_t nb_y, size_
         fclose(f);
         return total;
     }
-    const long long target = 4ll << 20; // cells per chunk
+    // cells per chunk (HYDRO_B200_CSV_CHUNK_CELLS overrides, e.g. to exercise many chunks)
+    long long target = 4ll << 20;
+    if (const char *env = getenv("HYDRO_B200_CSV_CHUNK_CELLS")) {
+        const long long v = atoll(env);
+        if (v > 0) target = v;
+    }
     const int rows = (int)std::max<long long>(1, std::min<long long>((long long)nb_x, target / per_row));
     const long long cap = per_row * rows;
     char *slots = nullptr, *out = nullptr, *host[2] = {nullptr, nullptr};

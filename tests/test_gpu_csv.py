@@ -83,3 +83,19 @@ def test_write_csv_matches_reference_program(cuda, prog, nb, T, steps, tmp_path)
     data = out.read_bytes()
     assert n == len(data)
     assert data == files[0].read_bytes()
+
+
+@pytest.mark.parametrize("chunk_cells", [7000, 150, 1])
+def test_write_csv_many_chunks(cuda, chunk_cells, tmp_path, monkeypatch):
+    """The chunked pipeline (format, scan, compact, double-buffered copy and write) gives
+    the same file whatever the chunk size: many chunks, one row per chunk, and chunks
+    smaller than a row (one row each)."""
+    nb, steps = (200, 150), 300
+    ref = _reference_csv("hydro", ["-x", "200", "-y", "150", "-t", "100", "-i", str(steps), "-w", str(steps)],
+                         tmp_path)
+    files = sorted(ref.glob(f"output_{steps}_*.csv"))
+    run = hb.BlastRun(nb, np.float64).run(1e9, steps)
+    monkeypatch.setenv("HYDRO_B200_CSV_CHUNK_CELLS", str(chunk_cells))
+    out = tmp_path / "gpu.csv"
+    hb.write_csv(run.cur, nb, out)
+    assert out.read_bytes() == files[0].read_bytes()
