@@ -224,7 +224,8 @@ typedef struct hydro_batch_status {
 } hydro_batch_status_t;
 
 /* A batch of `dim`-D (2) instances in FP32 (precision_bytes 4) or FP64 (8), rows per work
- * item `chunk` (0: default), at most `capacity` instances, on `stream` (NULL: its own). */
+ * item `chunk` (0: 32 rows in 2D, 64 planes in 3D), at most `capacity` instances, on `stream`
+ * (NULL: its own). */
 void *hydro_batch_create(int dim, int precision_bytes, int chunk, int capacity, void *stream);
 /* Allocate, initialise and admit one instance; returns its slot (>= 0) or an error code. */
 int hydro_batch_add(void *batch, const hydro_blast_t *spec);

@@ -528,7 +528,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
 
   public:
     BatchEngine(int chunk, int capacity, cudaStream_t stream, int *rc)
-        : chunk_(chunk > 0 ? chunk : (D == 2 ? 128 : 64)), cap_(capacity)
+        : chunk_(chunk > 0 ? chunk : (D == 2 ? 32 : 64)), cap_(capacity)
     {
         own_stream_ = (stream == nullptr);
         cudaError_t e = cudaSuccess;
