@@ -18,6 +18,8 @@ larger than L2, so no flush is needed between steps.
   variants   FP32 2D and FP64/FP32 3D 512^3 plain-path numbers (a few steps each)
 
 `--impl reference` times the reference's CPU kernel alone on the same metric.
+`--tour` instead times every kernel of the library on a small case (state above L2
+size), one JSON line per kernel with its GB/s against the measured copy bandwidth.
 Under torchrun (N>1) each rank runs its own replica (no data-path collective; weak
 scaling) and rank 0 prints the max-over-ranks timing.
 """
@@ -443,6 +445,110 @@ def bench_serving(hb, torch, rates=(10.0, 1000.0), nreq=8, seed=0, max_wall=20.0
     return res
 
 
+# ------------------------------------------------------------------- kernel tour ---
+def bench_tour(hb, torch, hbm, reps=5, log=print):
+    """Every kernel of the library on a case whose state is larger than L2 (126 MB), timed
+    with CUDA events on the launching stream: one JSON line per entry with the algorithmic
+    bytes of one call, its duration, GB/s and the fraction of the measured copy bandwidth.
+    Pair it with an `ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,...` launch
+    list of the same command for the DRAM bytes each kernel moves."""
+    from hydro_b200.autotune import _blasts
+    from hydro_b200.batch import Batch
+
+    lines = []
+    E = torch.cuda.Event
+
+    def timed(name, fn, nbytes, note="", stream=None):
+        st = stream or torch.cuda.current_stream()
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            a, b = E(enable_timing=True), E(enable_timing=True)
+            a.record(st)
+            fn()
+            b.record(st)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        m = statistics.median(ms)
+        gbs = nbytes / (m / 1e3) / 1e9
+        line = dict(tour=name, ms=m, bytes=int(nbytes), gb_s=gbs, frac=gbs / hbm, note=note)
+        lines.append(line)
+        log(json.dumps(line))
+
+    nb2, nb3 = (4000, 2000), (256, 256, 256)
+    for T, tn in ((np.float64, "double"), (np.float32, "float")):
+        isz = np.dtype(T).itemsize
+        # initial condition: writes every cell of both arrays (ghosts included)
+        for nb in (nb2, nb3):
+            d = len(nb)
+            phys = hb.Physics(T, nb)
+            st = hb.alloc_state(nb, T)
+            allc = int(np.prod([n + 2 for n in nb]))
+            timed(f"init{d}d_kernel<{tn}> {'x'.join(map(str, nb))}", lambda: hb.init_blast(st, phys),
+                  allc * (2 + d) * isz, "writes all cells of both arrays; first Dt fused")
+            cells = int(np.prod(nb))
+            timed(f"mass_kernel<{tn}> {'x'.join(map(str, nb))}", lambda: hb.mass(st[0], nb), cells * 2 * isz,
+                  "rho of the (rho, E) pairs: whole 32-byte sectors hold both")
+            # the one-thread-per-cell kernel (every face from both sides, as the reference)
+            nx = hb.alloc_state(nb, T)
+            dtd = phys.dtd(T(1e-5))
+            dt = torch.zeros(1, dtype=st[0].dtype, device="cuda")
+            timed(f"direct{d}d<{tn}> {'x'.join(map(str, nb))}",
+                  lambda: hb.step(st, nx, dt, phys, dtd, kernel=hb.KERNEL_DIRECT, sync=False),
+                  cells * 2 * (2 + d) * isz, "plus the redo2d/redo3d launch, which returns at once")
+            del st, nx
+            torch.cuda.empty_cache()
+        # the exact signal-speed pass: a calm state stepped after a fast one on the same
+        # Dt_next and grid skips every cell, so the redo pass recomputes the maximum
+        phys = hb.Physics(T, nb2)
+        fast, calm, nx = hb.alloc_state(nb2, T), hb.alloc_state(nb2, T), hb.alloc_state(nb2, T)
+        hb.init_blast(fast, phys)
+        hb.init_blast(calm, phys)
+        fast[0][1::2] *= 50.0
+        dtd = phys.dtd(T(1e-6))
+        dt = torch.zeros(1, dtype=fast[0].dtype, device="cuda")
+
+        def forced():
+            hb.step(fast, nx, dt, phys, dtd, kernel=hb.KERNEL_STRIP, sync=False)
+            hb.step(calm, nx, dt, phys, dtd, kernel=hb.KERNEL_STRIP, sync=False)
+
+        cells = int(np.prod(nb2))
+        timed(f"strip2d<{tn}> x2 + redo2d<{tn}> (forced) 4000x2000", forced, cells * (2 * 8 + 4) * isz,
+              "two steps (2 x 64 or 32 B per cell) and one redo pass reading the new state")
+        del fast, calm, nx
+        torch.cuda.empty_cache()
+        # batched engines: a run of 4 steps plus the conservation sums, as one graph
+        for d, n in ((2, 64), (3, 48)):
+            blasts = _blasts(d, n, 3)
+            s = torch.cuda.Stream()
+            b = Batch(d, T, capacity=n, stream=s)
+            for bl in blasts:
+                b.add(bl)
+            cells = sum(int(np.prod(bl.nb)) for bl in blasts)
+            timed(f"batch{d}d<{tn}> x4 + batch_sums ({n} instances, {cells / 1e6:.1f} M cells)",
+                  lambda: b.run(4, sync=False), cells * (4 * 2 * (2 + d) + (2 + d)) * isz,
+                  "4 steps and one conservation-sum pass", stream=s)
+            b.close()
+            torch.cuda.empty_cache()
+    # CSV output on the GPU: state in, text out (the file write overlaps the next chunk)
+    nbc = (2000, 1000)
+    for T in (np.float64,):
+        phys = hb.Physics(T, nbc)
+        st = hb.alloc_state(nbc, T)
+        hb.init_blast(st, phys)
+        with tempfile.TemporaryDirectory() as td:
+            out = Path(td) / "tour.csv"
+            nbytes = hb.write_csv(st, nbc, out)
+            timed("write_csv (format_lines + compact_lines + fwrite) 2000x1000 FP64",
+                  lambda: hb.write_csv(st, nbc, out), int(np.prod(nbc)) * 4 * 8 + nbytes,
+                  f"state read plus {nbytes / 1e6:.0f} MB of text written to a file")
+        del st
+        torch.cuda.empty_cache()
+    return lines
+
+
 # ------------------------------------------------------------------------ main ---
 def main():
     ap = argparse.ArgumentParser()
@@ -466,6 +572,8 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=8)
     ap.add_argument("--serving-wall", type=float, default=20.0, help="cap per serving run, seconds")
     ap.add_argument("--no-serving-plain", action="store_true")
+    ap.add_argument("--tour", action="store_true",
+                    help="time every kernel of the library on a small case (one JSON line each) and exit")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.nb != [40000, 20000], "at least 3 warm-up steps"
 
@@ -511,6 +619,12 @@ def main():
     max_over_ranks, barrier = reps.max_over_ranks, reps.barrier
 
     hbm, peak_kind = peaks()
+    if args.tour:
+        if rank == 0:
+            bench_tour(hb, torch, hbm, log=lambda m: print(m, flush=True))
+        reps.barrier()
+        reps.close()
+        return
     cells = int(np.prod(nb))
     isz = np.dtype(Tcase).itemsize
     bpc = BYTES_PER_CELL[(dim, isz)]
