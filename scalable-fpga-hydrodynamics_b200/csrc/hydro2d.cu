@@ -146,35 +146,55 @@ __global__ void __launch_bounds__(kStripNT, 4)
 // hydro2d/main.cxx:280-338: rho = u_in inside the circle of radius min(cx,cy)/3
 // centred at ((NB_X+1)/2, (NB_Y+1)/2) in ghost-shifted indices, u_out outside;
 // E = p/(gamma-1); zero momentum. First Dt = min over cells of C_min/(c_s + |u|).
+// The local Dt of a uniform state at rest: C_min / (c_s + |u|) with the reference's
+// per-cell operations (hydro2d/main.cxx:318-336), as the bits of a double.
+template <class T>
+__device__ __forceinline__ unsigned long long rest_dt_bits2(T ur, T uE, T C_min, T gamma, T gm1)
+{
+    using A = Ar<T>;
+    const T inv = A::rcp(ur);
+    const T qu = A::mul(T(0), inv), qv = A::mul(T(0), inv);
+    const T temp = A::add(A::mul(qu, qu), A::mul(qv, qv));
+    const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
+    const T qp = A::mul(A::mul(gm1, ur), e_int);
+    const T cs = A::sqrt(A::mul(A::mul(gamma, qp), inv));
+    const T un = A::sqrt(temp);
+    return (unsigned long long)__double_as_longlong((double)A::div(C_min, A::add(cs, un)));
+}
+
+// The circle splits the cells into two uniform states, so their energy p/(gamma-1) and
+// local Dt are evaluated once per thread for the states its cells hold, not once per
+// cell: the same operations on the same operands, hence the same bits. Per cell: the
+// distance test and the stores. Each thread covers the rows i = 1 + blockIdx.y + k *
+// gridDim.y of its column j.
 template <class T>
 __global__ void init2d_kernel(T *rhoE, T *uv, int nb_x, int nb_y, long long ys, double cx, double cy, double radius,
                               T u_in, T u_out, T p_in, T p_out, T C_min, T gamma, T gm1, unsigned long long *min_bits)
 {
     using A = Ar<T>;
     const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const T E_in = A::div(p_in, gm1), E_out = A::div(p_out, gm1);
+    bool any_in = false, any_out = false;
+    if (j <= nb_y) {
+        const double dy = __dsub_rn((double)j, cy), dy2 = __dmul_rn(dy, dy);
+        for (int i = 1 + blockIdx.y; i <= nb_x; i += gridDim.y) {
+            const double dx = __dsub_rn((double)i, cx);
+            const double d = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), dy2));
+            const bool in = d <= radius;
+            const long long c = (long long)i * ys + j;
+            rhoE[2 * c] = in ? u_in : u_out;
+            rhoE[2 * c + 1] = in ? E_in : E_out;
+            uv[2 * c] = T(0);
+            uv[2 * c + 1] = T(0);
+            any_in |= in;
+            any_out |= !in;
+        }
+    }
     unsigned long long best = ~0ull;
-    for (int i = 1 + blockIdx.y; i <= nb_x; i += gridDim.y) {
-        if (j > nb_y) break;
-        const double dx = __dsub_rn((double)i, cx), dy = __dsub_rn((double)j, cy);
-        const double d = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
-        const bool in = d <= radius;
-        const T ur = in ? u_in : u_out;
-        const T uE = A::div(in ? p_in : p_out, gm1);
-        const long long c = (long long)i * ys + j;
-        rhoE[2 * c] = ur;
-        rhoE[2 * c + 1] = uE;
-        uv[2 * c] = T(0);
-        uv[2 * c + 1] = T(0);
-        const T inv = A::rcp(ur);
-        const T qu = A::mul(T(0), inv), qv = A::mul(T(0), inv);
-        const T temp = A::add(A::mul(qu, qu), A::mul(qv, qv));
-        const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
-        const T qp = A::mul(A::mul(gm1, ur), e_int);
-        const T cs = A::sqrt(A::mul(A::mul(gamma, qp), inv));
-        const T un = A::sqrt(temp);
-        const T local = A::div(C_min, A::add(cs, un));
-        const unsigned long long bits = (unsigned long long)__double_as_longlong((double)local);
-        best = bits < best ? bits : best;
+    if (any_in) best = rest_dt_bits2(u_in, E_in, C_min, gamma, gm1);
+    if (any_out) {
+        const unsigned long long b = rest_dt_bits2(u_out, E_out, C_min, gamma, gm1);
+        best = b < best ? b : best;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -185,29 +205,10 @@ __global__ void init2d_kernel(T *rhoE, T *uv, int nb_x, int nb_y, long long ys, 
 }
 
 // ------------------------------------------------------------------ mass kernel ---
-template <class T>
-__global__ void mass_kernel(const T *rhoE, int nb_x, int nb_y, int nb_z, double2 *partials)
+// Warp-wide compensated merge in a fixed lane order; the result lands in every lane.
+__device__ __forceinline__ void warp_neumaier(double &s, double &c)
 {
-    // interior cells in row-major order; one compensated partial per block
-    const long long zs = nb_z > 0 ? nb_z + 2 : 1;
-    const long long ys = (long long)(nb_y + 2) * zs;
-    const long long ncol = (long long)nb_y * (nb_z > 0 ? nb_z : 1);
-    const long long n = (long long)nb_x * ncol;
-    double s = 0.0, c = 0.0;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-         q += (long long)gridDim.x * blockDim.x) {
-        const long long i = 1 + q / ncol, r = q % ncol;
-        long long cell;
-        if (nb_z > 0) cell = i * ys + (1 + r / nb_z) * zs + (1 + r % nb_z);
-        else cell = i * ys + 1 + r;
-        neumaier_add(s, c, (double)rhoE[2 * cell]);
-    }
-    StepAcc acc;
-    acc.ms = s;
-    acc.mc = c;
-    // reuse the epilogue's deterministic block combine through a private path
-    __shared__ double ss[32], sc[32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const double s2 = __shfl_xor_sync(0xffffffffu, s, o);
@@ -215,11 +216,41 @@ __global__ void mass_kernel(const T *rhoE, int nb_x, int nb_y, int nb_z, double2
         if (lane & o) {
             double a = s2, b = c2;
             neumaier_merge(a, b, s, c);
-            s = a; c = b;
+            s = a;
+            c = b;
         } else {
             neumaier_merge(s, c, s2, c2);
         }
     }
+}
+
+// Compensated sum of the interior density, one partial per block. Rows of interior
+// cells (2D: i; 3D: (i, j)) go to blocks in turn and their cells to the threads, so
+// each cell's address needs no division.
+template <class T>
+__global__ void mass_kernel(const T *rhoE, int nb_x, int nb_y, int nb_z, double2 *partials)
+{
+    const bool three = nb_z > 0;
+    const long long zs = three ? (long long)nb_z + 2 : 1;
+    const long long ys = (long long)(nb_y + 2) * zs;
+    const int nj = three ? nb_y : 1; // rows (i, j): j only in 3D
+    const int rowlen = three ? nb_z : nb_y;
+    const int step_i = (int)(gridDim.x / nj), step_j = (int)(gridDim.x % nj);
+    int i = (int)(blockIdx.x / nj), j = (int)(blockIdx.x % nj);
+    double s = 0.0, c = 0.0;
+    while (i < nb_x) {
+        const long long base = (1 + (long long)i) * ys + (three ? (1 + (long long)j) * zs : 0) + 1;
+        for (int t = threadIdx.x; t < rowlen; t += blockDim.x) neumaier_add(s, c, (double)rhoE[2 * (base + t)]);
+        i += step_i;
+        j += step_j;
+        if (j >= nj) {
+            j -= nj;
+            ++i;
+        }
+    }
+    __shared__ double ss[32], sc[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    warp_neumaier(s, c);
     if (lane == 0) { ss[warp] = s; sc[warp] = c; }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -228,12 +259,15 @@ __global__ void mass_kernel(const T *rhoE, int nb_x, int nb_y, int nb_z, double2
     }
 }
 
+// One warp: lane l merges partials l, l + 32, ... in order, then the lanes merge in a
+// fixed order (deterministic).
 __global__ void sum_partials_kernel(const double2 *partials, int n, double *out)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     double s = 0.0, c = 0.0;
-    for (int b = 0; b < n; ++b) neumaier_merge(s, c, partials[b].x, partials[b].y);
-    *out = __dadd_rn(s, c);
+    for (int b = threadIdx.x; b < n; b += 32) neumaier_merge(s, c, partials[b].x, partials[b].y);
+    warp_neumaier(s, c);
+    if (threadIdx.x == 0) *out = __dadd_rn(s, c);
 }
 
 // ----------------------------------------------------------------- host drivers ---
@@ -391,7 +425,9 @@ int init2d_at(T *rhoE, T *uv, size_t nb_x, size_t nb_y, double cx, double cy, do
     const T gm1 = gamma - T(1);
     cudaError_t e = cudaMemcpyAsync(bits, &init, sizeof init, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
-        const int gx = (int)((nb_y + 127) / 128), gy = (int)std::min<size_t>(nb_x, 65535);
+        // 16 blocks of 128 threads per SM; each thread takes nb_x / gy rows of its column
+        const int gx = (int)((nb_y + 127) / 128);
+        const int gy = (int)std::max<size_t>(1, std::min<size_t>({nb_x, 65535, (size_t)std::max(1, 148 * 16 / gx)}));
         init2d_kernel<T><<<dim3(gx, gy), 128, 0, stream>>>(rhoE, uv, (int)nb_x, (int)nb_y, ys > 0 ? ys : (long long)nb_y + 2, cx, cy,
                                                            radius, u_in, u_out, p_in, p_out, C_min, gamma, gm1, bits);
         e = cudaGetLastError();

@@ -129,7 +129,27 @@ template <class T> __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) st
 }
 
 // ------------------------------------------------------------- initial condition ---
-// hydro3d/main.cxx:296-363
+// hydro3d/main.cxx:296-363. The local Dt of a uniform state at rest, C_min/(c_s + |u|),
+// with the reference's per-cell operations, as the bits of a double.
+template <class T>
+__device__ __forceinline__ unsigned long long rest_dt_bits3(T ur, T uE, T C_min, T gamma, T gm1)
+{
+    using A = Ar<T>;
+    const T inv = A::rcp(ur);
+    const T q = A::mul(T(0), inv);
+    const T temp = A::add(A::add(A::mul(q, q), A::mul(q, q)), A::mul(q, q));
+    const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
+    const T qp = A::mul(A::mul(gm1, ur), e_int);
+    const T cs = A::sqrt(A::mul(A::mul(gamma, qp), inv));
+    const T un = A::sqrt(temp);
+    return (unsigned long long)__double_as_longlong((double)A::div(C_min, A::add(cs, un)));
+}
+
+// The sphere splits the cells into two uniform states: their energy p/(gamma-1) and
+// local Dt are evaluated once per thread for the states its cells hold (the same
+// operations on the same operands, so the same bits); per cell only the distance test
+// and the stores remain. Each thread covers the planes i = 1 + blockIdx.z + m * gridDim.z
+// of its column (j, k).
 template <class T>
 __global__ void init3d_kernel(T *rhoE, T *uvw, int nb_x, int nb_y, int nb_z, long long zs, long long zy, double cx,
                               double cy, double cz, double radius, T u_in, T u_out, T p_in, T p_out, T C_min,
@@ -138,32 +158,30 @@ __global__ void init3d_kernel(T *rhoE, T *uvw, int nb_x, int nb_y, int nb_z, lon
     using A = Ar<T>;
     const int k = 1 + blockIdx.x * 32 + threadIdx.x;
     const int j = 1 + blockIdx.y * 4 + threadIdx.y;
-    unsigned long long best = ~0ull;
+    const T E_in = A::div(p_in, gm1), E_out = A::div(p_out, gm1);
+    bool any_in = false, any_out = false;
     if (k <= nb_z && j <= nb_y) {
+        const double dy = __dsub_rn((double)j, cy), dz = __dsub_rn((double)k, cz);
+        const double dy2 = __dmul_rn(dy, dy), dz2 = __dmul_rn(dz, dz);
         for (int i = 1 + blockIdx.z; i <= nb_x; i += gridDim.z) {
-            const double dx = __dsub_rn((double)i, cx), dy = __dsub_rn((double)j, cy), dz = __dsub_rn((double)k, cz);
-            const double d =
-                __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+            const double dx = __dsub_rn((double)i, cx);
+            const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), dy2), dz2));
             const bool in = d <= radius;
-            const T ur = in ? u_in : u_out;
-            const T uE = A::div(in ? p_in : p_out, gm1);
             const long long c = (long long)i * zy + (long long)j * zs + k;
-            rhoE[2 * c] = ur;
-            rhoE[2 * c + 1] = uE;
+            rhoE[2 * c] = in ? u_in : u_out;
+            rhoE[2 * c + 1] = in ? E_in : E_out;
             uvw[3 * c] = T(0);
             uvw[3 * c + 1] = T(0);
             uvw[3 * c + 2] = T(0);
-            const T inv = A::rcp(ur);
-            const T q = A::mul(T(0), inv);
-            const T temp = A::add(A::add(A::mul(q, q), A::mul(q, q)), A::mul(q, q));
-            const T e_int = A::sub(A::mul(uE, inv), A::mul(A::half, temp));
-            const T qp = A::mul(A::mul(gm1, ur), e_int);
-            const T cs = A::sqrt(A::mul(A::mul(gamma, qp), inv));
-            const T un = A::sqrt(temp);
-            const T local = A::div(C_min, A::add(cs, un));
-            const unsigned long long bits = (unsigned long long)__double_as_longlong((double)local);
-            best = bits < best ? bits : best;
+            any_in |= in;
+            any_out |= !in;
         }
+    }
+    unsigned long long best = ~0ull;
+    if (any_in) best = rest_dt_bits3(u_in, E_in, C_min, gamma, gm1);
+    if (any_out) {
+        const unsigned long long b = rest_dt_bits3(u_out, E_out, C_min, gamma, gm1);
+        best = b < best ? b : best;
     }
     const int tl = threadIdx.x + 32 * threadIdx.y;
 #pragma unroll
@@ -318,7 +336,10 @@ int init3d_at(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, double cx,
     cudaError_t e = cudaMemcpyAsync(bits, &init, sizeof init, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
         const long long zs = (long long)nb_z + 2, zy = (long long)(nb_y + 2) * zs;
-        dim3 grid((unsigned)((nb_z + 31) / 32), (unsigned)((nb_y + 3) / 4), (unsigned)std::min<size_t>(nb_x, 65535));
+        // 16 blocks of 128 threads per SM; each thread takes nb_x / gz planes of its column
+        const size_t gxy = ((nb_z + 31) / 32) * ((nb_y + 3) / 4);
+        const size_t gz = std::max<size_t>(1, std::min<size_t>({nb_x, 65535, (size_t)148 * 16 / std::min<size_t>(gxy, 148 * 16)}));
+        dim3 grid((unsigned)((nb_z + 31) / 32), (unsigned)((nb_y + 3) / 4), (unsigned)gz);
         init3d_kernel<T><<<grid, dim3(32, 4), 0, stream>>>(rhoE, uvw, (int)nb_x, (int)nb_y, (int)nb_z, zs, zy, cx, cy,
                                                            cz, radius, u_in, u_out, p_in, p_out, C_min, gamma, gm1,
                                                            bits);
