@@ -148,38 +148,48 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
             x[4 * k3NT<T>] = pair3<T>(P.mw, P.eup_xy);
             x[5 * k3NT<T>] = pair3<T>(P.eup_z, T(0));
         }
-        Flux3<T> fxhi{};
-        if (m >= 1 && iwarp) fxhi = face_flux3(face3_x(Pm), face3_x(P), ph);
-
-        // faces of plane m-1 (an interior plane when 2 <= m)
-        if (m >= 2) {
-            // +y face of (j | j+1), from this lane's previous-plane cell and the warp above's
+        // +y face of (j | j+1), from this lane's previous-plane cell and the warp above's
+        auto yface = [&]() {
             const FaceIn3<T> me = face3_y(Pm);
-            Flux3<T> fy{};
-            if (w < k3Warps<T> - 1) {
-                const FaceIn3<T> nb = xp_face_y<T>(&S.xP[(m - 1) & 1][0][t + 32]);
-                FaceIn3<T> L = me, R = nb;
-                if (kEdge) {
-                    if (j == 0) L = mirror3(nb);
-                    if (j == g.nb_y) R = mirror3(me);
-                }
-                fy = face_flux3(L, R, ph);
-                S.xF[m & 1][0][t] = pair3<T>(fy.r, fy.n);
-                S.xF[m & 1][1][t] = pair3<T>(fy.t1, fy.t2);
-                S.xFE[m & 1][t] = fy.E;
+            const FaceIn3<T> nb = xp_face_y<T>(&S.xP[(m - 1) & 1][0][t + 32]);
+            FaceIn3<T> L = me, R = nb;
+            if (kEdge) {
+                if (j == 0) L = mirror3(nb);
+                if (j == g.nb_y) R = mirror3(me);
             }
-            // +z face of (k | k+1): the next lane's cell from the exchange buffer (lane 31
-            // reads the next warp's lane 0, a face no interior lane uses)
-            Flux3<T> fz{};
+            return face_flux3(L, R, ph);
+        };
+        // +z face of (k | k+1): the next lane's cell from the exchange buffer (lane 31
+        // reads the next warp's lane 0, a face no interior lane uses)
+        auto zface = [&]() {
+            const FaceIn3<T> mz = face3_z(Pm);
+            const FaceIn3<T> nz = xp_face_z<T>(&S.xP[(m - 1) & 1][0][t + 1]);
+            FaceIn3<T> L = mz, R = nz;
+            if (kEdge) {
+                if (k == 0) L = mirror3(nz);
+                if (k == g.nb_z) R = mirror3(mz);
+            }
+            return face_flux3(L, R, ph);
+        };
+        auto publish_y = [&](const Flux3<T> &fy) {
+            S.xF[m & 1][0][t] = pair3<T>(fy.r, fy.n);
+            S.xF[m & 1][1][t] = pair3<T>(fy.t1, fy.t2);
+            S.xFE[m & 1][t] = fy.E;
+        };
+        Flux3<T> fxhi{};
+        if (m >= 2) {
+            // faces of plane m-1 (an interior plane when 2 <= m): the warps holding interior
+            // rows evaluate their x, y and z faces together (independent work the compiler
+            // can interleave); the halo row above them only its +y face
+            Flux3<T> fy{}, fz{};
             if (iwarp) {
-                const FaceIn3<T> mz = face3_z(Pm);
-                const FaceIn3<T> nz = xp_face_z<T>(&S.xP[(m - 1) & 1][0][t + 1]);
-                FaceIn3<T> L = mz, R = nz;
-                if (kEdge) {
-                    if (k == 0) L = mirror3(nz);
-                    if (k == g.nb_z) R = mirror3(mz);
-                }
-                fz = face_flux3(L, R, ph);
+                fxhi = face_flux3(face3_x(Pm), face3_x(P), ph);
+                fy = yface();
+                fz = zface();
+                publish_y(fy);
+            } else if (w < k3Warps<T> - 1) {
+                fy = yface();
+                publish_y(fy);
             }
             __syncthreads(); // +y faces of this plane published
             if (iwarp) {
@@ -204,6 +214,7 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
                 }
             }
         } else {
+            if (m >= 1 && iwarp) fxhi = face_flux3(face3_x(Pm), face3_x(P), ph);
             __syncthreads(); // keep one barrier per plane: publishes this plane's xP
         }
         fxlo = fxhi;
