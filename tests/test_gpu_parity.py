@@ -166,6 +166,34 @@ def test_fp32_accuracy_vs_fp64_oracle(cuda, oracle, nb, steps):
             assert l1 <= 1e-5
 
 
+def interior(a, nb, nv):
+    return a.reshape(tuple(n + 2 for n in nb) + (nv,))[tuple(slice(1, n + 1) for n in nb)]
+
+
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+@pytest.mark.parametrize("nb", [(1, 1), (6000, 1000), (3, 4000), (2500, 64), (1, 1, 1), (128, 128, 128),
+                                (300, 5, 70), (7, 33, 65)])
+def test_initial_condition_and_mass(cuda, oracle, nb, T):
+    """Device blast IC and first Dt against the oracle, byte for byte, on grids where one
+    thread covers many rows (planes) of its column and where it covers one; the device mass
+    sum against the oracle's, on the same grids (many rows per block, 3D row stepping)."""
+    phys = hb.Physics(T, nb)
+    st = hb.alloc_state(nb, T)
+    dt = hb.init_blast(st, phys)
+    ref = tuple(np.zeros(a.numel(), dtype=T) for a in st)
+    dref = oracle.init(ref, phys)
+    assert T(dt).tobytes() == T(dref).tobytes()
+    nv = 3 if len(nb) == 3 else 2
+    for a, r, k in zip(st, ref, (2, nv)):
+        assert interior(a.cpu().numpy(), nb, k).tobytes() == interior(r, nb, k).tobytes()
+    m, mref = hb.mass(st[0], nb), oracle.mass(ref[0], nb)
+    assert abs(m - mref) <= 1e-14 * abs(mref)
+    # a seeded state (every cell different) through the mass sum
+    rnd = seeded_state(nb, T, 3)
+    m2 = hb.mass(cuda.from_numpy(rnd[0].copy()).cuda(), nb)
+    assert abs(m2 - oracle.mass(rnd[0], nb)) <= 1e-14 * abs(oracle.mass(rnd[0], nb))
+
+
 def test_mass_conservation(cuda):
     for nb in ((60, 60), (40, 30, 20)):
         run = hb.BlastRun(nb, np.float64).run(2.0, 200)
