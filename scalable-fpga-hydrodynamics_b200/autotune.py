@@ -1,7 +1,8 @@
 """Tile-shape autotuner for the batched step, keyed on dimensionality and precision.
 
 The batched kernels take a fixed block shape (2D: 128 lanes over 126 interior columns;
-3D: 8 x 32 lanes over 6 x 30 interior columns) and one free tile parameter: the number
+3D: 8 x 32 lanes over 6 x 30 interior columns in FP64, 16 x 32 over 14 x 30 in FP32) and
+one free tile parameter: the number
 of X rows (planes) a work item marches, `chunk`. Longer chunks re-read fewer halo rows
 and take fewer work items; shorter ones balance uneven instances better. `tune` times a
 seeded mini-batch of the batched workload for each candidate and keeps the fastest;
