@@ -402,7 +402,7 @@ def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=
     return out
 
 
-def bench_serving(hb, torch, rates=(10.0, 1000.0), nreq=8, seed=0, max_wall=20.0, plain=True, log=print):
+def bench_serving(hb, torch, rates=(10.0, 100.0, 1000.0), nreq=8, seed=0, max_wall=20.0, plain=True, log=print):
     """The serving workload: Poisson streams of mixed requests (70% 2D sides [128, 4096],
     30% 3D sides [32, 256], t_end in [0.05, 0.5] of the sound-crossing time, FP32/FP64 50/50),
     `nreq` requests per rate, through the continuous-batching server (150 GB budget) and
@@ -568,7 +568,7 @@ def main():
     ap.add_argument("--batched-steps", type=int, default=200)
     ap.add_argument("--batched-chunk", type=int, default=0, help="rows per work item (0: autotuned)")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serving-rates", type=float, nargs="+", default=[10.0, 1000.0])
+    ap.add_argument("--serving-rates", type=float, nargs="+", default=[10.0, 100.0, 1000.0])
     ap.add_argument("--serving-requests", type=int, default=8)
     ap.add_argument("--serving-wall", type=float, default=20.0, help="cap per serving run, seconds")
     ap.add_argument("--no-serving-plain", action="store_true")
