@@ -1,5 +1,6 @@
 """Host-side logic without a GPU: the seeded workloads, the serving summary, and the
-replica bookkeeping over a world of two gloo ranks on CPU."""
+replica bookkeeping and the X-slab ghost exchange over worlds of two and three gloo ranks
+on CPU."""
 from __future__ import annotations
 
 import math
@@ -144,3 +145,73 @@ def test_slab_rows_partition():
             assert max(sizes) - min(sizes) <= 1 and min(sizes) >= 1
     with pytest.raises(hb.HydroError):
         slab_rows(2, 3, 0)
+
+
+def _slab_rank_main(rank, world, port, nb, q):
+    """One gloo rank: fill its slab with values naming (global row, column, component),
+    exchange the X ghost rows and report what landed in them, plus the MIN of Dt."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    try:
+        import torch
+
+        from conftest import load_pkg as _load
+
+        _load()
+        from hydro_b200.replicas import Replicas
+        from hydro_b200.slabs import XSlabRun, slab_rows
+
+        reps = Replicas("gloo", timeout_s=60)
+        run = XSlabRun.__new__(XSlabRun)  # the exchange and Dt logic only: no device state
+        run.torch, run.reps, run.nb, run.T = torch, reps, tuple(nb), np.float64
+        run.lo, run.hi = slab_rows(nb[0], world, rank)
+        n = run.hi - run.lo + 1
+        run.nb_local = (n,) + tuple(nb[1:])
+        run.row = int(np.prod([m + 2 for m in nb[1:]]))
+        arrays = []
+        for nv in (2, len(nb)):
+            a = np.full((n + 2, run.row, nv), -1.0)
+            for i in range(1, n + 1):
+                g = run.lo + i - 1
+                a[i] = g * 1e4 + np.arange(run.row)[:, None] * 10 + np.arange(nv)[None, :]
+            arrays.append(torch.from_numpy(a.reshape(-1).copy()))
+        run.cur = tuple(arrays)
+        run.exchange()
+        ghosts = [(a.numpy().reshape(n + 2, run.row, -1)[0].copy(), a.numpy().reshape(n + 2, run.row, -1)[n + 1].copy())
+                  for a in run.cur]
+        dt = run._min(0.25 + rank)
+        reps.barrier()
+        reps.close()
+        q.put((rank, run.lo, run.hi, ghosts, float(dt)))
+    except Exception as e:  # reported to the parent
+        q.put((rank, repr(e), None, None, None))
+
+
+@pytest.mark.parametrize("world,nb", [(2, (6, 5)), (3, (7, 4)), (2, (4, 3, 2)), (3, (5, 2, 3))])
+def test_slab_exchange_gloo(world, nb):
+    """The X-slab ghost exchange across gloo ranks on CPU: ghost row 0 of each rank holds
+    the last interior row of the rank on its left and ghost row NB+1 the first row of the
+    rank on its right, periodically (with two ranks both neighbours are the same peer);
+    the next Dt is the MIN over ranks."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_slab_rank_main, args=(r, world, port, nb, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted((q.get(timeout=120) for _ in procs), key=lambda o: o[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    row = int(np.prod([m + 2 for m in nb[1:]]))
+    for rank, lo, hi, ghosts, dt in out:
+        assert ghosts is not None, lo
+        assert dt == 0.25
+        left = lo - 1 if lo > 1 else nb[0]    # global row below this slab (periodic)
+        right = hi + 1 if hi < nb[0] else 1   # global row above it
+        for (g0, g1), nv in zip(ghosts, (2, len(nb))):
+            cols = np.arange(row)[:, None] * 10 + np.arange(nv)[None, :]
+            np.testing.assert_array_equal(g0, left * 1e4 + cols)
+            np.testing.assert_array_equal(g1, right * 1e4 + cols)
