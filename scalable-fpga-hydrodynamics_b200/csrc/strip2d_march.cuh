@@ -32,11 +32,13 @@ template <class T> struct Smem2 {
     using V2 = typename Vec2<T>::type;
     __align__(128) V2 sr[kStages][kStripNT]; // (rho, E) rows
     __align__(128) V2 su[kStages][kStripNT]; // (rho u, rho v) rows
-    // y-face inputs of every lane's cell (lane t at [t]) and every lane's right face
-    // flux (lane t at [t+1]), as pairs so that each lane moves them with 128-bit (FP64)
-    // or 64-bit (FP32) shared-memory accesses
-    __align__(16) V2 xP[4][kStripNT + 1];
-    __align__(16) V2 xF[2][kStripNT + 1];
+    // y-face inputs of every lane's cell (lane t at [t]) and every lane's right face flux
+    // (lane t at [t+1]), as pairs so that each lane moves them with 128-bit (FP64) or 64-bit
+    // (FP32) shared-memory accesses. Both are double-buffered by row parity, which leaves one
+    // barrier per row: a lane may publish row n's inputs while its neighbour still reads row
+    // n-1's, and the fluxes of row n-1 are read after row n's barrier.
+    __align__(16) V2 xP[2][4][kStripNT + 1];
+    __align__(16) V2 xF[2][2][kStripNT + 1];
     __align__(8) uint64_t full[kStages];
     int abort;
 };
@@ -96,7 +98,7 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
 
     Cell2<T> Pm{};
     T Ur = 0, Uu = 0, Uv = 0, UE = 0;
-    Flux2<T> fxlo{}, fyl{}, fyr{};
+    Flux2<T> fxlo{}, fyr{};
     int m = 0;
 #pragma unroll 2
     for (; m < nrows; ++m) {
@@ -112,12 +114,14 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
         const bool yrow = (m >= 1) && (m <= nrows - 2);
         if (yrow) {
             const FaceIn<T> me = face_y(P);
-            S.xP[0][t] = mk2<T>(me.r, me.un);
-            S.xP[1][t] = mk2<T>(me.p, me.Ka);
-            S.xP[2][t] = mk2<T>(me.iKa, me.mn);
-            S.xP[3][t] = mk2<T>(me.mt, me.eup);
+            S.xP[m & 1][0][t] = mk2<T>(me.r, me.un);
+            S.xP[m & 1][1][t] = mk2<T>(me.p, me.Ka);
+            S.xP[m & 1][2][t] = mk2<T>(me.iKa, me.mn);
+            S.xP[m & 1][3][t] = mk2<T>(me.mt, me.eup);
         }
-        __syncthreads(); // stage s consumed by every lane; y-face inputs published
+        // stage s consumed by every lane; this row's y-face inputs and the previous row's
+        // right-face fluxes published
+        __syncthreads();
         if (S.abort) break;
         if (t == 0 && m + kStages < nrows) issue(m + kStages);
 
@@ -125,6 +129,9 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
             // x face (row n-1 | row n) of this column; then the update of row n-1
             const Flux2<T> fxhi = face_flux(face_x(Pm), face_x(P), ph);
             if (m >= 2 && interior) {
+                // row n-1's left face is lane t-1's right face of that row
+                const V2 f0 = S.xF[(m - 1) & 1][0][t], f1 = S.xF[(m - 1) & 1][1][t];
+                const Flux2<T> fyl{f0.x, f0.y, f1.x, f1.y};
                 const Upd2<T> o = update2(Ur, Uu, Uv, UE, fxlo, fxhi, fyl, fyr, DtDx, DtDy, ph);
                 const long long c = (long long)(g.i0 + m - 2) * g.ys + j;
                 reinterpret_cast<V2 *>(rhoE_n)[c] = mk2<T>(o.r, o.E);
@@ -136,7 +143,8 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
         if (yrow) {
             // y face (j | j+1) of row n, from this lane's cell and the next lane's
             const FaceIn<T> me = face_y(P);
-            const V2 n0 = S.xP[0][t + 1], n1 = S.xP[1][t + 1], n2 = S.xP[2][t + 1], n3 = S.xP[3][t + 1];
+            const V2 n0 = S.xP[m & 1][0][t + 1], n1 = S.xP[m & 1][1][t + 1], n2 = S.xP[m & 1][2][t + 1],
+                     n3 = S.xP[m & 1][3][t + 1];
             FaceIn<T> L = me;
             FaceIn<T> R{n0.x, n0.y, n1.x, n1.y, n2.x, n2.y, n3.x, n3.y};
             if (wall_warp) {
@@ -144,11 +152,8 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
                 if (j == g.nb_y) R = mirror(me); // wall at j = NB_Y + 1/2
             }
             fyr = face_flux(L, R, ph);
-            S.xF[0][t + 1] = mk2<T>(fyr.r, fyr.n);
-            S.xF[1][t + 1] = mk2<T>(fyr.t, fyr.E);
-            __syncthreads(); // right faces published: lane t's left face is lane t-1's right
-            const V2 f0 = S.xF[0][t], f1 = S.xF[1][t];
-            fyl = Flux2<T>{f0.x, f0.y, f1.x, f1.y};
+            S.xF[m & 1][0][t + 1] = mk2<T>(fyr.r, fyr.n);
+            S.xF[m & 1][1][t + 1] = mk2<T>(fyr.t, fyr.E);
         }
         Pm = P;
         Ur = a.x; Uu = b.x; Uv = b.y; UE = a.y;
