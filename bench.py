@@ -575,7 +575,6 @@ def main():
     ap.add_argument("--tour", action="store_true",
                     help="time every kernel of the library on a small case (one JSON line each) and exit")
     args = ap.parse_args()
-    assert args.warmup >= 3 or args.nb != [40000, 20000], "at least 3 warm-up steps"
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -608,6 +607,8 @@ def main():
         print(json.dumps(line), flush=True)
         return
 
+    # the timed GPU runs of the full-size workload take at least 3 warm-up steps
+    assert args.warmup >= 3 or args.nb != [40000, 20000] or args.tour, "at least 3 warm-up steps"
     import torch
 
     hb = load_pkg()
