@@ -2,12 +2,13 @@
 // chunk per block) and the batched step (batch3d, tiles of many instances per persistent
 // block).
 //
-// One block of 8 warps covers an 8 (y) x 32 (z) tile of columns starting at (jbase,
-// kbase): 6 x 30 interior columns plus a one-cell halo ring. Each lane copies its own
-// cell of each X plane into a k3Stages-deep shared-memory ring with cp.async (any
-// alignment of the interleaved pairs/triples), converts it to primitives once and
-// publishes them as 16-byte pairs (double-buffered by plane parity; one barrier per
-// plane). Per plane a lane computes one x face (registers), one z face (the next lane's
+// One block of 8 (FP64) or 16 (FP32) warps covers a (warps) y x 32 z tile of columns
+// starting at (jbase, kbase): the interior columns plus a one-cell halo ring. Each X plane
+// of the tile is copied into a k3Stages-deep shared-memory ring with cp.async (any
+// alignment of the interleaved pairs/triples): in FP64 by every lane for its own cell, in
+// FP32 by the two halo-row warps for the whole tile. Each lane converts its cell to
+// primitives once and publishes them as 16-byte pairs (double-buffered by plane parity;
+// one barrier per plane). Per plane a lane computes one x face (registers), one z face (the next lane's
 // cell from shared memory, the flux back by shuffles) and one y face (the warp above's
 // cell, the flux back through shared memory), then updates the plane behind it. Every
 // updated interior cell is handed to `sink`.
