@@ -6,6 +6,7 @@ from __future__ import annotations
 import math
 import os
 import socket
+import time
 
 import numpy as np
 import pytest
@@ -215,3 +216,88 @@ def test_slab_exchange_gloo(world, nb):
             cols = np.arange(row)[:, None] * 10 + np.arange(nv)[None, :]
             np.testing.assert_array_equal(g0, left * 1e4 + cols)
             np.testing.assert_array_equal(g1, right * 1e4 + cols)
+
+
+class _FakeEngine:
+    """Stands in for a batch engine: each instance needs `max_steps` steps, occupies
+    100 bytes per cell, and `run(n)` advances every active instance by up to n steps (the
+    engine's device-side end condition stops an instance at exactly its need)."""
+
+    def __init__(self, log):
+        self.log, self.slots, self.next = log, {}, 0
+
+    def bytes(self, blast):
+        return 100 * int(np.prod(blast.nb))
+
+    def add(self, blast):
+        self.next += 1
+        self.slots[self.next] = [blast, 0]
+        self.log.append(("add", id(self), self.next, self.bytes(blast)))
+        return self.next
+
+    def run(self, n, sync=True):
+        time.sleep(0.001)  # a tick takes time, so later arrivals meet running work
+        for s in self.slots.values():
+            s[1] = min(s[1] + n, s[0].max_steps)
+
+    def sync(self):
+        pass
+
+    def status(self, slot):
+        b, steps = self.slots[slot]
+        return {"active": steps < b.max_steps, "steps": steps, "err": 0}
+
+    def remove(self, slot):
+        self.log.append(("remove", id(self), slot, self.bytes(self.slots[slot][0])))
+        del self.slots[slot]
+
+    def state(self, slot):
+        return None
+
+    def close(self):
+        pass
+
+
+def test_server_admission_on_cpu():
+    """The continuous-batching loop with fake engines: first-come first-served admission,
+    the memory budget never exceeded, a request that can never fit rejected, requests that
+    arrive while others run admitted at once when room allows, and every admitted request
+    retired after exactly the steps it needs."""
+    from hydro_b200.batch import Blast
+    from hydro_b200.serving import Server
+    from hydro_b200.workloads import Request
+
+    log = []
+    srv = Server.__new__(Server)  # the scheduling loop only: no device
+    srv.budget, srv.steps_per_tick, srv.engines, srv.streams = 100 * 10_000.0, 4, {}, {}
+
+    def engine(dim, dtype):
+        key = (dim, np.dtype(dtype).name)
+        if key not in srv.engines:
+            srv.engines[key] = _FakeEngine(log)
+        return srv.engines[key]
+
+    srv.engine = engine
+    sizes = [(60, 60), (50, 40), (90, 90), (20, 30, 10), (200, 200), (10, 10), (40, 40, 4)]
+    need = [9, 30, 13, 5, 3, 21, 7]
+    reqs = [Request(rid=i, arrival=0.0005 * i, blast=Blast(nb=nb, max_steps=n),
+                    dtype=np.float32 if i % 2 else np.float64)
+            for i, (nb, n) in enumerate(zip(sizes, need))]
+    recs, wall = srv.serve(reqs, max_wall=30.0)
+    recs = {r.rid: r for r in recs}
+    # (200, 200) needs 4 MB against a 1 MB budget: rejected, never admitted
+    assert recs[4].err == -1 and recs[4].admit is None and recs[4].done is None
+    for r in reqs:
+        if r.rid != 4:
+            assert recs[r.rid].done is not None and recs[r.rid].steps == r.blast.max_steps, r.rid
+    # memory in use never above the budget
+    used = peak = 0
+    for ev, _eng, _slot, nbytes in log:
+        used += nbytes if ev == "add" else -nbytes
+        peak = max(peak, used)
+    assert peak <= srv.budget and used == 0
+    # admission in arrival order
+    admitted = [rid for rid in sorted(recs, key=lambda k: recs[k].admit or 1e30) if recs[rid].admit is not None]
+    assert admitted == sorted(admitted)
+    # continuous batching: the second request joined while the first was still running
+    assert recs[1].admit < recs[0].done
