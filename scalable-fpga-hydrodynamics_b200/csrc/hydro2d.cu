@@ -25,6 +25,7 @@
 //            evaluated from both sides like the reference. Any alignment, any size;
 //            used when the strip kernel's TMA rules do not hold and as a cross-check.
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <stddef.h>
 #include <stdio.h>
@@ -114,24 +115,26 @@ template <class T> __global__ void __launch_bounds__(kRedoNT) redo2d(Args2<T> g)
 }
 
 // ------------------------------------------------------------------- strip kernel ---
-template <class T>
+// kTma: rows staged by TMA tile loads (16-byte row pitch), else by per-lane cp.async.
+template <class T, bool kTma>
 __global__ void __launch_bounds__(kStripNT, 4)
     strip2d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args2<T> g)
 {
     __shared__ Smem2<T> S;
-    if (threadIdx.x == 0) {
+    if (kTma && threadIdx.x == 0) {
         prefetch_tensormap(&tmr);
         prefetch_tensormap(&tmu);
     }
     march2d_init(S);
     const int i0 = 1 + g.chunk * (int)blockIdx.y;
-    const March2 geo{kStripW * (int)blockIdx.x, i0, min(i0 + g.chunk - 1, g.nb_x), g.nb_x, g.nb_y, g.ys, g.xwrap};
+    const March2 geo{kStripW * (int)blockIdx.x, i0, min(i0 + g.chunk - 1, g.nb_x), g.nb_x, g.nb_y, g.ys, g.xwrap,
+                     g.rhoE, g.uv};
     StepAcc acc;
     const float tlof = skip_threshold_f(g.scr, g.key);
     const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
     const Phys<T> ph = g.ph;
     unsigned ld = 0;
-    const bool ok = march2d<T>(S, &tmr, &tmu, geo, g.rhoE_n, g.uv_n, ph, g.DtDx, g.DtDy, ld, [&](const Upd2<T> &o) {
+    const bool ok = march2d<T, kTma>(S, &tmr, &tmu, geo, g.rhoE_n, g.uv_n, ph, g.DtDx, g.DtDy, ld, [&](const Upd2<T> &o) {
         acc.add_mass(o.r);
         const float fu = (float)o.u, fv = (float)o.v;
         if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1, tlo2))
@@ -322,15 +325,21 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
 
     using V2 = typename Vec2<T>::type;
     const size_t rowbytes = 2 * sizeof(T) * (nb_y + 2);
-    bool strip_ok = aligned(rhoE, 16) && aligned(uv, 16) && aligned(rhoE_next, sizeof(V2)) &&
-                    aligned(uv_next, sizeof(V2)) && rowbytes % 16 == 0;
+    // the strip kernel stages rows by TMA when the arrays are 16-byte aligned and the row
+    // pitch a multiple of 16 bytes, else by per-lane cp.async (cells aligned to their size)
+    bool tma_ok = aligned(rhoE, 16) && aligned(uv, 16) && aligned(rhoE_next, sizeof(V2)) &&
+                  aligned(uv_next, sizeof(V2)) && rowbytes % 16 == 0;
     CUtensorMap tmr, tmu;
-    if (strip_ok && which != Kernel::Direct) {
-        strip_ok = encode_tmap_2d(&tmr, tmap_type<T>(), rhoE, 2 * (nb_y + 2), nb_x + 2, rowbytes, 2 * kStripNT, 1) &&
-                   encode_tmap_2d(&tmu, tmap_type<T>(), uv, 2 * (nb_y + 2), nb_x + 2, rowbytes, 2 * kStripNT, 1);
+    std::memset(&tmr, 0, sizeof tmr);
+    std::memset(&tmu, 0, sizeof tmu);
+    if (tma_ok && which != Kernel::Direct) {
+        tma_ok = encode_tmap_2d(&tmr, tmap_type<T>(), rhoE, 2 * (nb_y + 2), nb_x + 2, rowbytes, 2 * kStripNT, 1) &&
+                 encode_tmap_2d(&tmu, tmap_type<T>(), uv, 2 * (nb_y + 2), nb_x + 2, rowbytes, 2 * kStripNT, 1);
     }
+    const bool strip_ok = tma_ok || (aligned(rhoE, sizeof(V2)) && aligned(uv, sizeof(V2)) &&
+                                     aligned(rhoE_next, sizeof(V2)) && aligned(uv_next, sizeof(V2)));
     if (which == Kernel::Strip && !strip_ok) {
-        set_error(kErrArg, "step2d: strip kernel needs 16-byte aligned arrays and rows");
+        set_error(kErrArg, "step2d: strip kernel needs arrays aligned to their cell size");
         return kErrArg;
     }
     const bool use_strip = strip_ok && which != Kernel::Direct;
@@ -352,7 +361,10 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
         nblocks = (unsigned)nstrips * (unsigned)nchunks;
         if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
         g.partials = ctx->partials;
-        strip2d<T><<<dim3(nstrips, nchunks), kStripNT, 0, stream>>>(tmr, tmu, g);
+        if (tma_ok)
+            strip2d<T, true><<<dim3(nstrips, nchunks), kStripNT, 0, stream>>>(tmr, tmu, g);
+        else
+            strip2d<T, false><<<dim3(nstrips, nchunks), kStripNT, 0, stream>>>(tmr, tmu, g);
     } else {
         const int gx = (int)((nb_y + kDirectNT - 1) / kDirectNT);
         const int gy = (int)std::min<size_t>(nb_x, 65535);
@@ -625,7 +637,7 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
         chunk = std::max(chunk, (NB_X + std::min<size_t>(max_chunks, 65535) - 1) / std::min<size_t>(max_chunks, 65535));
         nchunks = (NB_X + chunk - 1) / chunk;
         g.chunk = (int)chunk;
-        strip2d<T><<<dim3((unsigned)nstrips, (unsigned)nchunks), kStripNT, 0, st>>>(tmr, tmu, g);
+        strip2d<T, true><<<dim3((unsigned)nstrips, (unsigned)nchunks), kStripNT, 0, st>>>(tmr, tmu, g);
         kernel = (int)Kernel::Strip;
     } else {
         const size_t gy = std::max<size_t>(1, std::min<size_t>({NB_X, 65535, kNoAllocMaxBlocks / gx_direct}));

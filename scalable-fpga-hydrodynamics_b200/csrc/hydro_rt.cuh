@@ -125,6 +125,25 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, in
                  : "memory");
 }
 
+// Per-thread asynchronous copy global -> shared of 4, 8 or 16 bytes (zero-filled when
+// !valid); completion by commit groups, waited on by the issuing thread.
+__device__ __forceinline__ void cp_async(void *dst, const void *src, int bytes, bool valid)
+{
+    const uint32_t d = smem_u32(dst);
+    const int n = valid ? bytes : 0;
+    if (bytes == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap *tm)
 {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tm)) : "memory");

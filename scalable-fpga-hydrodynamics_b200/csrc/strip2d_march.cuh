@@ -59,12 +59,18 @@ struct March2 {
     int nb_x, nb_y;
     long long ys;
     int xwrap; // X neighbours of rows 1 and NB_X by periodic wrap (1) or ghost rows (0)
+    // the input arrays, read directly by the per-lane loads (rows whose pitch TMA rejects)
+    const void *in_r = nullptr, *in_u = nullptr;
 };
 
 // kEdge = false: a strip whose every lane holds a real column (1 <= j <= NB_Y), so no
 // unit-state substitution and no wall face that an interior lane uses; kEdge = true: any
 // strip. Returns false when a bounded barrier wait gave up (the block then stops).
-template <bool kEdge, class T, class Sink>
+// kTma = true: each row of each array arrives by one TMA tile load issued by thread 0
+// (16-byte row pitch). kTma = false: each lane copies its own cell with cp.async (any
+// pitch; 8-byte (FP32) or 16-byte (FP64) aligned arrays), so a lane reads only what it
+// copied and the ring needs no barrier.
+template <bool kEdge, bool kTma, class T, class Sink>
 __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tmr, const CUtensorMap *tmu,
                                               const March2 &g, T *rhoE_n, T *uv_n, const Phys<T> &ph, T DtDx,
                                               T DtDy, unsigned &ld, Sink &sink)
@@ -93,8 +99,24 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
         tma_load_2d(&S.sr[s][0], tmr, xcoord, row, &S.full[s]);
         tma_load_2d(&S.su[s][0], tmu, xcoord, row, &S.full[s]);
     };
-    if (t == 0)
-        for (int m = 0; m < kStages && m < nrows; ++m) issue(m);
+    // per-lane form: this lane's cell of row m into its slot of stage (ld0 + m) % kStages
+    const bool in_row = !kEdge || j <= g.nb_y + 1;
+    auto issue_lane = [&](int m) {
+        const int s = (ld0 + (unsigned)m) % kStages;
+        if (m < nrows) {
+            const int row = g.xwrap ? wrap_row(g.i0 - 1 + m, g.nb_x) : g.i0 - 1 + m;
+            const long long c = in_row ? (long long)row * g.ys + j : 0;
+            cp_async(&S.sr[s][t], static_cast<const V2 *>(g.in_r) + c, (int)sizeof(V2), in_row);
+            cp_async(&S.su[s][t], static_cast<const V2 *>(g.in_u) + c, (int)sizeof(V2), in_row);
+        }
+        cp_async_commit();
+    };
+    if constexpr (kTma) {
+        if (t == 0)
+            for (int m = 0; m < kStages && m < nrows; ++m) issue(m);
+    } else {
+        for (int m = 0; m < kStages - 1; ++m) issue_lane(m);
+    }
 
     Cell2<T> Pm{};
     T Ur = 0, Uu = 0, Uv = 0, UE = 0;
@@ -104,7 +126,12 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
     for (; m < nrows; ++m) {
         const unsigned q = ld0 + (unsigned)m;
         const int s = q % kStages;
-        if (!mbar_wait_bounded(&S.full[s], (q / kStages) & 1)) S.abort = 1;
+        if constexpr (kTma) {
+            if (!mbar_wait_bounded(&S.full[s], (q / kStages) & 1)) S.abort = 1;
+        } else {
+            issue_lane(m + kStages - 1); // into the slot this lane read for row m-1
+            cp_async_wait<kStages - 1>(); // this lane's copy of row m landed
+        }
         V2 a = S.sr[s][t], b = S.su[s][t];
         if (kEdge && !real_col) {
             a = mk2<T>(T(1), T(1));
@@ -123,7 +150,7 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
         // right-face fluxes published
         __syncthreads();
         if (S.abort) break;
-        if (t == 0 && m + kStages < nrows) issue(m + kStages);
+        if (kTma && t == 0 && m + kStages < nrows) issue(m + kStages);
 
         if (m >= 1) {
             // x face (row n-1 | row n) of this column; then the update of row n-1
@@ -159,6 +186,7 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
         Ur = a.x; Uu = b.x; Uv = b.y; UE = a.y;
     }
     ld = ld0 + (unsigned)nrows;
+    if constexpr (!kTma) cp_async_wait<0>();
     if (m < nrows) {
         // gave up on a barrier: wait (bounded) for the loads still in flight before the
         // block's shared memory is released
@@ -173,14 +201,14 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
 
 // One strip march: the lean form away from the Y walls, the general one at them (the
 // choice is uniform over the block).
-template <class T, class Sink>
+template <class T, bool kTma = true, class Sink>
 __device__ __forceinline__ bool march2d(Smem2<T> &S, const CUtensorMap *tmr, const CUtensorMap *tmu, const March2 &g,
                                         T *rhoE_n, T *uv_n, const Phys<T> &ph, T DtDx, T DtDy, unsigned &ld,
                                         Sink &&sink)
 {
     if (g.jbase >= 1 && g.jbase + kStripNT - 1 <= g.nb_y)
-        return march2d_strip<false>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
-    return march2d_strip<true>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
+        return march2d_strip<false, kTma>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
+    return march2d_strip<true, kTma>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
 }
 
 } // namespace hydro

@@ -31,23 +31,6 @@ constexpr int k3Stages = 4;
 
 __device__ __forceinline__ int wrap_plane(int n, int nb_x) { return n == 0 ? nb_x : (n == nb_x + 1 ? 1 : n); }
 
-__device__ __forceinline__ void cp_async(void *dst, const void *src, int bytes, bool valid)
-{
-    const uint32_t d = smem_u32(dst);
-    const int n = valid ? bytes : 0;
-    if (bytes == 16)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-    else if (bytes == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 template <class T> __device__ __forceinline__ typename Vec2<T>::type pair3(T a, T b)
 {
     typename Vec2<T>::type v;

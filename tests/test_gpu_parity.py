@@ -48,10 +48,7 @@ def test_step2d_bitwise(cuda, oracle, nb, T, kernel):
         ref = (np.zeros_like(st[0]), np.zeros_like(st[1]))
         dtd = phys.dtd(cfl_dt(phys, seed))
         dref = oracle.step(st, ref, phys, dtd)
-        if kernel == hb.KERNEL_STRIP and T is np.float32 and (nb[1] + 2) % 2:
-            with pytest.raises(hb.HydroError):
-                gpu_step(cuda, st, phys, dtd, kernel)
-            continue
+        # FP32 with odd NB_Y: a row pitch TMA rejects, staged by per-lane copies instead
         out, d, info = gpu_step(cuda, st, phys, dtd, kernel)
         assert info.kernel == kernel
         assert d.tobytes() == dref.tobytes()
