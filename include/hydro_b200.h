@@ -60,10 +60,13 @@ typedef struct hydro_step_info {
     double mass;      /* compensated FP64 sum of the new interior density */
     double max_speed; /* max over interior cells of c_s + |u| (Dt_next = C_min / this) */
     unsigned err;     /* bit 0: non-physical state; bit 1: a bounded wait timed out */
-    int kernel;       /* 1 = TMA strip kernel, 2 = direct kernel */
+    int kernel;       /* 1 = strip kernel (rows by TMA, or per-lane cp.async where TMA rejects the
+                         row pitch), 2 = direct kernel */
 } hydro_step_info_t;
 
-/* Kernel selection for the *_step entry points */
+/* Kernel selection for the *_step entry points. AUTO takes the strip kernel whenever the
+ * input and output arrays are aligned to their cell size, else the direct kernel; STRIP
+ * on arrays that are not returns HYDRO_ERR_ARG. */
 #define HYDRO_KERNEL_AUTO 0
 #define HYDRO_KERNEL_STRIP 1
 #define HYDRO_KERNEL_DIRECT 2
