@@ -1,5 +1,6 @@
 // Device runtime pieces shared by the 2D and 3D kernels:
-//  - mbarrier / TMA (cp.async.bulk.tensor) inline-PTX wrappers, every wait bounded;
+//  - mbarrier / TMA (cp.async.bulk.tensor) inline-PTX wrappers, every wait bounded, and
+//    the per-thread cp.async copies used where TMA's alignment rules do not fit;
 //  - the fused end-of-step reduction: the CFL maximum signal speed (the reference
 //    folds it serially, hydro2d/kernel.cxx:313 and :318) and an FP64 compensated sum of
 //    the new density (the mass the reference sums on the host in long double,
