@@ -261,20 +261,33 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def has_avx2_fma():
+def cpu_flags():
     try:
-        flags = Path("/proc/cpuinfo").read_text()
-        return " avx2" in flags and " fma" in flags
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("flags"):
+                return set(line.split(":", 1)[1].split())
     except Exception:
-        return False
+        pass
+    return set()
+
+
+def has_avx2_fma():
+    f = cpu_flags()
+    return {"avx2", "fma", "bmi2"} <= f
+
+
+def has_avx512():
+    """The x86-64-v4 level: AVX-512 F, BW, CD, DQ and VL."""
+    return {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= cpu_flags()
 
 
 def cpu_reference_sample(nb_y: int, rows: int, seconds: float, threads: int):
     """The reference's own kernel.cxx (oracle/_ref, FMA-contracting build as in the
-    reference Makefile) on `threads` host threads, each stepping its own rows x nb_y
+    reference Makefile, at the highest instruction-set level the host supports) on
+    `threads` host threads, each stepping its own rows x nb_y
     slab of the blast (the reference's X-slab decomposition, one slab per core) for
     about `seconds`. Falls back to the oracle restatement when oracle/_ref is absent.
-    Returns (cell-updates/s, kind, description)."""
+    Returns (cell-updates/s, kind, description, timed seconds)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
 
@@ -285,7 +298,10 @@ def cpu_reference_sample(nb_y: int, rows: int, seconds: float, threads: int):
     phys.nb = nb
     o = orc.Oracle()
     kind = "reference"
-    if orc.available_ref(2, T, fast=True) and has_avx2_fma():
+    if orc.available_ref(2, T, fast=True, level="v4") and has_avx512():
+        stepper = orc.RefKernel(2, T, fast=True, level="v4").step
+        what = "oracle/_ref/libref2d_f64_fast_v4.so (reference kernel.cxx, -O2 -march=x86-64-v4)"
+    elif orc.available_ref(2, T, fast=True) and has_avx2_fma():
         stepper = orc.RefKernel(2, T, fast=True).step
         what = "oracle/_ref/libref2d_f64_fast.so (reference kernel.cxx, -O2 -march=x86-64-v3)"
     elif orc.available_ref(2, T):
@@ -325,7 +341,7 @@ def cpu_reference_sample(nb_y: int, rows: int, seconds: float, threads: int):
     for th in ths:
         th.join()
     cells = (c1 - c0) * rows * nb_y
-    return cells / (t1 - t0), kind, what
+    return cells / (t1 - t0), kind, what, t1 - t0
 
 
 # --------------------------------------------------------------- batched / serving ---
@@ -443,6 +459,63 @@ def bench_serving(hb, torch, rates=(10.0, 100.0, 1000.0), nreq=8, seed=0, max_wa
         res[f"rate_{rate:g}"] = entry
         log(f"serving rate {rate:g}/s: {json.dumps(entry)}")
     return res
+
+
+# ------------------------------------------------------------ FP32 vs FP64 accuracy ---
+def fp32_accuracy(hb, torch, nb, steps=100):
+    """The plain path in FP32 and in FP64 from the same blast for `steps` iterations;
+    relative L1 (sum |a - b| / sum |b|) and L-infinity (max |a - b| / max |b|) of rho, p
+    and the velocities of the FP32 result against the FP64 one, which is bit-identical
+    to the reference's FP64 kernel (the GPU parity tests)."""
+    dim = len(nb)
+    runs = {}
+    for T in (np.float64, np.float32):
+        r = hb.BlastRun(nb, T).run(float("inf"), steps)
+        runs[T] = r
+    gm1 = 0.4
+    out = dict(steps=steps, grid="x".join(map(str, nb)), reference="plain FP64 path (bit-identical to the oracle)")
+    names = ["rho", "p", "u", "v", "w"][:dim + 2]
+    acc = {n: [0.0, 0.0, 0.0, 0.0] for n in names}  # sum|d|, sum|b|, max|d|, max|b|
+    nplane = int(np.prod([n + 2 for n in nb[1:]]))
+    inner = tuple(slice(1, n + 1) for n in nb[1:])
+    nv = dim
+    rows = max(1, int(2e8 // nplane))
+    for i0 in range(1, nb[0] + 1, rows):
+        i1 = min(nb[0] + 1, i0 + rows)
+        fields = {}
+        for T, r in runs.items():
+            rhoE = r.cur[0][2 * nplane * i0:2 * nplane * i1].double().view(i1 - i0, *[n + 2 for n in nb[1:]], 2)
+            mom = r.cur[1][nv * nplane * i0:nv * nplane * i1].double().view(i1 - i0, *[n + 2 for n in nb[1:]], nv)
+            rho = rhoE[(slice(None),) + inner + (0,)]
+            E = rhoE[(slice(None),) + inner + (1,)]
+            m = mom[(slice(None),) + inner]
+            vel = m / rho.unsqueeze(-1)
+            p = gm1 * (E - 0.5 * (m * vel).sum(-1))
+            fields[T] = [rho, p] + [vel[..., c] for c in range(nv)]
+        for n, a, b in zip(names, fields[np.float32], fields[np.float64]):
+            d = (a - b).abs()
+            acc[n][0] += float(d.sum())
+            acc[n][1] += float(b.abs().sum())
+            acc[n][2] = max(acc[n][2], float(d.max()))
+            acc[n][3] = max(acc[n][3], float(b.abs().max()))
+    for n, (sd, sb, md, mb) in acc.items():
+        out[n] = dict(rel_l1=sd / sb if sb > 0 else 0.0, rel_linf=md / mb if mb > 0 else 0.0)
+    del runs
+    torch.cuda.empty_cache()
+    return out
+
+
+def config_for(nb, T):
+    """The workload description both arms print (identical dicts)."""
+    dim = len(nb)
+    isz = np.dtype(T).itemsize
+    bpc = BYTES_PER_CELL[(dim, isz)]
+    cells = int(np.prod(nb))
+    return dict(workload=(f"{dim}D blast {'x'.join(map(str, nb))} {'FP64' if isz == 8 else 'FP32'}, "
+                          f"plain path (one launcher call per step)"),
+                nb=list(nb), bytes_per_cell_update=bpc,
+                l2=f"inputs larger than L2 ({cells * bpc / 2 / 1e9:.1f} GB state, 126 MB L2): no flush",
+                parallelism="replicas: one per GPU, no data-path collective")
 
 
 # ------------------------------------------------------------------- kernel tour ---
@@ -567,6 +640,9 @@ def main():
     ap.add_argument("--batched-instances", type=int, default=256)
     ap.add_argument("--batched-steps", type=int, default=200)
     ap.add_argument("--batched-chunk", type=int, default=0, help="rows per work item (0: autotuned)")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=100,
+                    help="iterations of the FP32-vs-FP64 accuracy runs on the large grids")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-rates", type=float, nargs="+", default=[10.0, 100.0, 1000.0])
     ap.add_argument("--serving-requests", type=int, default=8)
@@ -582,26 +658,35 @@ def main():
     dim = int(args.case[0])
     Tcase = np.float64 if args.case.endswith("f64") else np.float32
     nb = tuple(args.nb) if len(args.nb) == dim else ((512, 512, 512) if dim == 3 else (40000, 20000))
-    workload = (f"{dim}D blast {'x'.join(map(str, nb))} {'FP64' if Tcase is np.float64 else 'FP32'}, "
-                f"plain path (one launcher call per step)")
 
     if args.impl == "reference":
         if rank != 0:
             return
+        if dim != 2 or Tcase is not np.float64:
+            print(json.dumps(dict(impl="reference", unavailable="the CPU reference arm times the 2D FP64 case")))
+            return
         thr = cpu_threads()
         rows = 32
-        per_step = []
+        per_step, secs = [], []
         for k in range(args.warmup + args.steps):
-            rate, kind, what = cpu_reference_sample(nb[1], rows, 2.0 if k >= args.warmup else 0.5, thr)
+            rate, kind, what, el = cpu_reference_sample(nb[1], rows, 2.0 if k >= args.warmup else 0.5, thr)
             if k >= args.warmup:
                 per_step.append(rate)
+                secs.append(el)
         rate = statistics.median(per_step)
         v = rate / 1e9
-        sample = f"{thr} threads x {rows}x{nb[1]} slabs of the blast, ~2 s per step ({what})"
+        timed = sum(secs)
+        sample = (f"{thr} threads x {rows}x{nb[1]} slabs of the blast, ~2 s per step ({what}); "
+                  f"value = the sample's cell-updates/s")
         line = dict(metric=METRIC, value=v, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
-                    ms_per_step=nb[0] * nb[1] / rate * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None,
+                    ms_per_step=timed / args.steps * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None,
                     dtype="f64", data="synthetic (reference blast IC)", impl="reference",
-                    config=dict(workload=workload, nb_x=nb[0], nb_y=nb[1], l2="inputs larger than L2"),
+                    config=config_for(nb, Tcase),
+                    extrapolated=dict(value=True, timed_region_s=timed,
+                                      sample_cells_per_step=thr * rows * nb[1],
+                                      full_grid_ms_per_step_at_this_rate=int(np.prod(nb)) / rate * 1e3,
+                                      note="each timed step is a ~2 s sample of the workload on every host "
+                                           "core; a full-grid step is not run"),
                     cpu_baseline=dict(value=v, unit=UNIT, cores=thr, kind=kind, sample=sample),
                     e2e=dict(value=v, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
         print(json.dumps(line), flush=True)
@@ -676,10 +761,16 @@ def main():
             nst = max(5, args.steps // 3)
             vc = int(np.prod(vnb))
             km = statistics.mean(vr["kernel_ms"])
-            bpc = BYTES_PER_CELL[(len(vnb), np.dtype(T).itemsize)]
+            vbpc = BYTES_PER_CELL[(len(vnb), np.dtype(T).itemsize)]
             variants[name] = dict(value=world * vc * nst / (vms / 1e3) / 1e9, unit=UNIT,
-                                  kernel_gbs=vc * bpc / (km / 1e3) / 1e9, frac=vc * bpc / (km / 1e3) / 1e9 / hbm,
+                                  kernel_gbs=vc * vbpc / (km / 1e3) / 1e9, frac=vc * vbpc / (km / 1e3) / 1e9 / hbm,
                                   kernel=int(vr["kernel"]), ms_per_step=vms / nst, clocks=vclocks)
+
+    accuracy = {}
+    if rank == 0 and world == 1 and not args.no_accuracy and args.case == "2d_f64":
+        # the FP32 plain path against FP64 on the large grids, 100 iterations each
+        for name, vnb in (("2d_40000x20000", nb), ("3d_512^3", (512, 512, 512))):
+            accuracy[name] = fp32_accuracy(hb, torch, vnb, steps=args.accuracy_steps)
 
     log = lambda msg: print(msg, file=sys.stderr, flush=True)
     batched = serving = None
@@ -696,7 +787,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and dim == 2:
         thr = cpu_threads()
-        rate, kind, what = cpu_reference_sample(nb[1], 32, 3.0, thr)
+        rate, kind, what, _el = cpu_reference_sample(nb[1], 32, 3.0, thr)
         cpu = dict(value=rate / 1e9, unit=UNIT, cores=thr, kind=kind,
                    sample=f"{thr} threads x 32x{nb[1]} slabs of the blast for 3 s ({what})")
 
@@ -704,12 +795,32 @@ def main():
         line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                     ms_per_step=ms_step, higher_is_better=True, scaling="weak", vs_baseline=None,
                     dtype="f64" if isz == 8 else "f32", data="synthetic (reference blast IC, built on the device)",
-                    config=dict(workload=workload, nb=list(nb),
-                                l2=f"inputs larger than L2 ({cells * bpc / 2 / 1e9:.1f} GB state, 126 MB L2)",
-                                parallelism=f"replicas x{world}"),
-                    roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps * r["launches_per_step"],
-                    clocks=clocks, energy=energy_entry(r["energy_j"], total_ms / 1e3, cells * args.steps),
-                    variants=variants, batched=batched, serving=serving)
+                    config=config_for(nb, Tcase), gpu_launches=args.steps * r["launches_per_step"],
+                    e2e=e2e, roofline=roofline, cpu_baseline=cpu, clocks=clocks)
+        # the metric's own quantities, compact, ahead of the detailed records
+        if batched:
+            line["batched_fp32_gcell_s"] = batched["batched_fp32"]["value"]
+            line["batched_fp64_gcell_s"] = batched["batched_fp64"]["value"]
+            line["batched_fp32_over_plain_fp64_same_instances"] = batched["batched_fp32_over_plain_fp64"]
+            line["batched_fp32_over_plain_fp64_large_grid"] = batched["batched_fp32"]["value"] / value
+            line["batched_fp32_rho_rel_l1_vs_fp64"] = batched["batched_fp32"]["rho_rel_l1_vs_fp64_max"]
+        if serving:
+            top = serving[max(serving, key=lambda k: float(k.split("_")[1]))]
+            line["serving"] = {k: dict(p50_s=v["batched"]["p50_s"], p99_s=v["batched"]["p99_s"],
+                                       completed=v["batched"]["completed"], gcell_s=v["batched"]["gcell_s"],
+                                       over_plain=v.get("batched_over_plain")) for k, v in serving.items()}
+            if "batched_fp32_over_plain_fp64" in top:
+                line["serving_fp32_over_plain_fp64_top_rate"] = top["batched_fp32_over_plain_fp64"]
+        if variants:
+            line["variants_gcell_s"] = {k: v["value"] for k, v in variants.items()}
+            line["variants_frac"] = {k: v["frac"] for k, v in variants.items()}
+        if accuracy:
+            line["fp32_vs_fp64"] = {k: {n: v[n] for n in ("rho", "p", "u", "v", "w") if n in v}
+                                    for k, v in accuracy.items()}
+        line["energy"] = energy_entry(r["energy_j"], total_ms / 1e3, cells * args.steps)
+        line["variants"] = variants
+        line["batched"] = batched
+        line["serving_detail"] = serving
         print(json.dumps(line), flush=True)
     reps.barrier()
     reps.close()

@@ -153,14 +153,37 @@ int hydro3d_step_f32(const float *d_rhoE, const float *d_uvw, float *d_rhoE_next
  * the library, which every GPU that loads the library holds until the process exits.
  * Limit: at most 65536 blocks of partial sums per launch, i.e. NB_Y <= 8257536 (larger
  * grids are rejected with HYDRO_ERR_ARG and a message); NB_X is handled by longer chunks.
- * The first call on a device performs a one-time set-up (it looks up the array's device
- * address); make that first call before any stream capture begins. All calls share the
- * array: calls that overlap on the GPU (two streams, two threads) race and must be
- * serialised by the caller. Arguments, results and return codes as hydro2d_step_f64. */
+ * The first call in a CUDA context performs a one-time set-up (it looks up the array's
+ * address in that context); make that first call before any stream capture begins. All
+ * calls share the array and it keeps the last call's contents: calls that overlap on the
+ * GPU (two streams, two threads) race and must be serialised by the caller.
+ * Arguments as hydro2d_step_f64 except that there is no `kernel` argument: the kernel is
+ * chosen as HYDRO_KERNEL_AUTO does, and the X ghost rows are always the in-kernel periodic
+ * wrap (HYDRO_X_GHOSTS_FROM_MEMORY is not available). With sync = 1 it waits and returns
+ * results and codes as hydro2d_step_f64; with sync = 0 it only enqueues, and the step's
+ * results and error codes come from hydro2d_noalloc_last_info. */
 int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv, double *d_rhoE_next, double *d_uv_next,
                              double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma,
                              double K, size_t NB_X, size_t NB_Y, double DtDx, double DtDy, void *stream, int sync,
                              hydro_step_info_t *info);
+
+/* Results of the last hydro2d_step_f64_noalloc call in the current CUDA context, read from
+ * the fixed array without allocating: the copy is ordered on `stream` (the step's stream),
+ * which it synchronises. Returns HYDRO_OK, HYDRO_ERR_NONPHYSICAL or HYDRO_ERR_TIMEOUT from
+ * the step's error bits. No counterpart in the reference. */
+int hydro2d_noalloc_last_info(void *stream, hydro_step_info_t *info);
+
+/* The launch shape hydro2d_step_f64_noalloc uses on a GPU with `sms` multiprocessors, for
+ * the strip kernel (strip = 1) or the direct kernel (0): rows per block (*chunk, 0 for the
+ * direct kernel) and the grid. Returns the number of blocks (at most 65536), or 0 when the
+ * grid does not fit the fixed scratch. Host only. No counterpart in the reference. */
+unsigned hydro2d_noalloc_launch_shape(size_t NB_X, size_t NB_Y, int strip, int sms, int *chunk, unsigned *grid_x,
+                                      unsigned *grid_y);
+
+/* Diagnostics: the number of per-device contexts (scratch words, partial sums, a pinned
+ * status record) the regular entry points have created in this process. The
+ * allocation-free entry points create none. No counterpart in the reference. */
+int hydro_device_contexts(void);
 
 /* Results of the last step launched on the current device, for steps enqueued with
  * sync = 0: valid once the caller has synchronised that step's stream. Returns

@@ -145,9 +145,11 @@ class RefKernel:
     """The reference's own kernel.cxx (unchanged, strict IEEE order) as a shared
     object exporting `launcher`; the SYCL stand-in runs its single_task inline."""
 
-    def __init__(self, dim: int, dtype, fast: bool = False):
+    def __init__(self, dim: int, dtype, fast: bool = False, level: str = ""):
+        """fast: the reference Makefile's -O2 with FMA contraction (x86-64-v3, or the
+        instruction-set level `level`, e.g. "v4"); else strict IEEE order."""
         T = np.dtype(dtype).type
-        suf = ("f64" if T is np.float64 else "f32") + ("_fast" if fast else "")
+        suf = ("f64" if T is np.float64 else "f32") + ("_fast" if fast else "") + (f"_{level}" if level else "")
         path = REF_DIR / f"libref{dim}d_{suf}.so"
         if not path.exists():
             raise FileNotFoundError(path)
@@ -172,8 +174,8 @@ class RefKernel:
         return self.T(dt[0])
 
 
-def available_ref(dim: int, dtype, fast: bool = False) -> bool:
-    suf = ("f64" if np.dtype(dtype) == np.float64 else "f32") + ("_fast" if fast else "")
+def available_ref(dim: int, dtype, fast: bool = False, level: str = "") -> bool:
+    suf = ("f64" if np.dtype(dtype) == np.float64 else "f32") + ("_fast" if fast else "") + (f"_{level}" if level else "")
     return (REF_DIR / f"libref{dim}d_{suf}.so").exists()
 
 

@@ -55,8 +55,12 @@ class StepInfo(ctypes.Structure):
 
 
 def build(force: bool = False) -> None:
-    """Compile the CUDA library in-tree (sm_100a) with the package Makefile."""
-    if LIB_PATH.exists() and not force:
+    """Compile the CUDA library in-tree (sm_100a) with the package Makefile. The make is
+    incremental: it rebuilds whatever is older than its sources and headers, so a kernel
+    edited since the last build is never run from a stale binary. Where no CUDA compiler
+    is installed (a machine that only runs a prebuilt tree) an existing library is used."""
+    nvcc = Path(os.environ.get("CUDA", "/usr/local/cuda")) / "bin" / "nvcc"
+    if not nvcc.exists() and LIB_PATH.exists() and not force:
         return
     subprocess.run(["make", "-C", str(PKG_DIR), "-j8"] + (["-B"] if force else []), check=True)
 

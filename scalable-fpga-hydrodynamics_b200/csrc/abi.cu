@@ -249,6 +249,8 @@ int hydro_last_step_info(hydro_step_info_t *info)
     return (st.err & kErrNonPhysical) ? kErrPhys : kOk;
 }
 
+int hydro_device_contexts(void) { return ctx_count(); }
+
 int hydro_last_error(void) { return last_error(); }
 const char *hydro_last_error_string(void) { return last_error_string(); }
 void hydro_clear_error(void) { clear_error(); }

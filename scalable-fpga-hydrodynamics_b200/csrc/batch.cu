@@ -542,7 +542,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
         if (e == cudaSuccess) e = cudaHostAlloc(&status_h_, sizeof(SlotStatus) * cap_, cudaHostAllocMapped);
         if (e == cudaSuccess) e = cudaHostGetDevicePointer(&status_d_, status_h_, 0);
         if (e == cudaSuccess) memset(status_h_, 0, sizeof(SlotStatus) * cap_);
-        int dev = 0, nsm = 148, occ = 1;
+        int dev = 0, nsm = 1, occ = 1;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         if constexpr (D == 2) {
@@ -973,7 +973,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
     SlotStatus *status_h_ = nullptr, *status_d_ = nullptr;
     std::vector<Slot> slots_;
     std::vector<int2> host_ranges_;
-    int nitems_ = 0, blocks_ = 148, sum_blocks_ = 148, graph_steps_ = -1, smem_ = 0;
+    int nitems_ = 0, blocks_ = 1, sum_blocks_ = 1, graph_steps_ = -1, smem_ = 0;
     cudaGraphExec_t graph_ = nullptr;
 };
 

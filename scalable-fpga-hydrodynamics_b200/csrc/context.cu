@@ -1,4 +1,5 @@
 // Per-device contexts, error latch and TMA descriptor encoding.
+#include <atomic>
 #include <cudaTypedefs.h>
 #include <mutex>
 #include <stdarg.h>
@@ -81,6 +82,26 @@ DevCtx *ctx_current(int *err)
     g_ctx[dev] = c;
     *err = kOk;
     return c;
+}
+
+int device_sms()
+{
+    static std::atomic<int> cache[64];
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n > 0) return n;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 1;
+    cache[dev].store(n, std::memory_order_relaxed);
+    return n;
+}
+
+int ctx_count()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    int n = 0;
+    for (DevCtx *c : g_ctx) n += (c != nullptr);
+    return n;
 }
 
 int ctx_reserve(DevCtx *c, size_t n)

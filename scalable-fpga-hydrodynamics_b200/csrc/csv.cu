@@ -365,7 +365,7 @@ long long write_csv(const T *rhoE, const T *uvx, size_t nb_x, size_t nb_y, size_
     for (long long row0 = 1; e == cudaSuccess && row0 <= (long long)nb_x; row0 += rows, ++chunk) {
         const int nr = (int)std::min<long long>(rows, (long long)nb_x - row0 + 1);
         const long long n = per_row * nr;
-        const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+        const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)device_sms() * 16);
         format_lines<T, D><<<blocks, 256, 0, st>>>(rhoE, uvx, (int)nb_y, (int)nb_z, row0, nr, (long long)i_offset,
                                                     slots, lens);
         e = cudaGetLastError();
@@ -476,7 +476,7 @@ int hydro_format_g(const double *d_values, size_t n, char *d_out, void *stream)
     int rc = ensure_pow5(st);
     if (rc != kOk) return rc;
     if (n == 0) return kOk;
-    format_values<<<(int)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(d_values, (long long)n, d_out);
+    format_values<<<(int)std::min<size_t>((n + 255) / 256, (size_t)device_sms() * 16), 256, 0, st>>>(d_values, (long long)n, d_out);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {

@@ -348,7 +348,7 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
     unsigned nblocks;
     if (use_strip) {
         const int nstrips = (int)((nb_y + kStripW - 1) / kStripW);
-        const int target = 148 * 3 * 8;
+        const int target = device_sms() * 3 * 8;
         int nchunks = (target + nstrips - 1) / nstrips;
         int chunk = (int)((nb_x + nchunks - 1) / nchunks);
         chunk = std::min(256, std::max(16, chunk));
@@ -381,7 +381,7 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
         return kErrCuda;
     }
     ctx->last_kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
-    const unsigned redo_blocks = 148 * 4;
+    const unsigned redo_blocks = (unsigned)device_sms() * 4;
     if (!sync) {
         // enqueued unconditionally; returns at once unless the step asked for it
         redo2d<T><<<redo_blocks, kRedoNT, 0, stream>>>(g);
@@ -439,7 +439,7 @@ int init2d_at(T *rhoE, T *uv, size_t nb_x, size_t nb_y, double cx, double cy, do
     if (e == cudaSuccess) {
         // 16 blocks of 128 threads per SM; each thread takes nb_x / gy rows of its column
         const int gx = (int)((nb_y + 127) / 128);
-        const int gy = (int)std::max<size_t>(1, std::min<size_t>({nb_x, 65535, (size_t)std::max(1, 148 * 16 / gx)}));
+        const int gy = (int)std::max<size_t>(1, std::min<size_t>({nb_x, 65535, (size_t)std::max(1, device_sms() * 16 / gx)}));
         init2d_kernel<T><<<dim3(gx, gy), 128, 0, stream>>>(rhoE, uv, (int)nb_x, (int)nb_y, ys > 0 ? ys : (long long)nb_y + 2, cx, cy,
                                                            radius, u_in, u_out, p_in, p_out, C_min, gamma, gm1, bits);
         e = cudaGetLastError();
@@ -485,7 +485,7 @@ template <class T> int mass_sum(const T *rhoE, size_t nb_x, size_t nb_y, size_t 
     int err;
     DevCtx *ctx = ctx_current(&err);
     if (!ctx) return err;
-    const int nb = 148 * 8;
+    const int nb = device_sms() * 8;
     if ((err = ctx_reserve(ctx, nb + 1)) != kOk) return err;
     double *dres = reinterpret_cast<double *>(ctx->partials + nb);
     mass_kernel<T><<<nb, 256, 0, s>>>(rhoE, (int)nb_x, (int)nb_y, (int)nb_z, ctx->partials);
@@ -532,32 +532,101 @@ static_assert(sizeof(StepScratch) + sizeof(StepStatus) <= kNoAllocHeader, "heade
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
+// The array's device address differs per CUDA context (a device's primary context, or a
+// context the caller created with the driver API), so it is looked up once per context
+// and kept with the kernel the context's last step ran.
+struct NoAllocEntry {
+    CUcontext ctx;
+    unsigned char *base;
+    int last_kernel;
+};
 std::mutex g_noalloc_mu;
-unsigned char *g_noalloc_dev[64] = {};
+NoAllocEntry g_noalloc[128];
+int g_noalloc_n = 0;
 
-// Device address of g_noalloc_scratch on the current device, looked up once per device.
-unsigned char *noalloc_scratch(int *rc)
+CUcontext current_context()
+{
+    using Fn = CUresult (*)(CUcontext *);
+    static Fn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<Fn>(p);
+    });
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
+
+// The entry of the current context, created (address looked up) on its first use.
+NoAllocEntry *noalloc_entry(const char *who, int *rc)
 {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= 64) {
-        set_error(kErrCuda, "hydro2d_step_f64_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "%s: cudaGetDevice failed: %s", who, cudaGetErrorString(e));
         *rc = kErrCuda;
         return nullptr;
     }
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_dev[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            set_error(kErrCuda, "hydro2d_step_f64_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-            *rc = kErrCuda;
-            return nullptr;
+    CUcontext ctx = current_context();
+    for (int i = 0; ctx && i < g_noalloc_n; ++i)
+        if (g_noalloc[i].ctx == ctx) {
+            *rc = kOk;
+            return &g_noalloc[i];
         }
-        g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch); // makes the device's context current if none was
+    if (e != cudaSuccess || !p) {
+        set_error(kErrCuda, "%s: cudaGetSymbolAddress failed: %s", who, cudaGetErrorString(e));
+        *rc = kErrCuda;
+        return nullptr;
     }
+    ctx = current_context();
+    for (int i = 0; ctx && i < g_noalloc_n; ++i)
+        if (g_noalloc[i].ctx == ctx) {
+            *rc = kOk;
+            return &g_noalloc[i];
+        }
+    if (!ctx || g_noalloc_n == (int)(sizeof g_noalloc / sizeof g_noalloc[0])) {
+        set_error(kErrCuda, "%s: no current CUDA context, or too many contexts", who);
+        *rc = kErrCuda;
+        return nullptr;
+    }
+    g_noalloc[g_noalloc_n] = NoAllocEntry{ctx, static_cast<unsigned char *>(p), 0};
     *rc = kOk;
-    return g_noalloc_dev[dev];
+    return &g_noalloc[g_noalloc_n++];
+}
+
+// Launch shape of the allocation-free step: the strip kernel's grid as step2d sizes it,
+// with the chunk grown until the blocks fit the fixed partials, or the direct kernel's
+// grid capped the same way. Returns the number of blocks, 0 if the grid cannot fit.
+unsigned noalloc_shape(size_t nb_x, size_t nb_y, bool strip, int sms, int *chunk, unsigned *gx, unsigned *gy)
+{
+    if (nb_x == 0 || nb_y == 0 || sms <= 0) return 0;
+    if (strip) {
+        const size_t nstrips = (nb_y + kStripW - 1) / kStripW;
+        if (nstrips > kNoAllocMaxBlocks) return 0;
+        const size_t max_chunks = std::min<size_t>(kNoAllocMaxBlocks / nstrips, 65535);
+        const size_t target = (size_t)sms * 3 * 8;
+        size_t nchunks = (target + nstrips - 1) / nstrips;
+        size_t c = std::min<size_t>(256, std::max<size_t>(16, (nb_x + nchunks - 1) / nchunks));
+        c = std::max(c, (nb_x + max_chunks - 1) / max_chunks);
+        nchunks = (nb_x + c - 1) / c;
+        *chunk = (int)c;
+        *gx = (unsigned)nstrips;
+        *gy = (unsigned)nchunks;
+    } else {
+        const size_t gxd = (nb_y + kDirectNT - 1) / kDirectNT;
+        if (gxd > kNoAllocMaxBlocks) return 0;
+        *chunk = 0;
+        *gx = (unsigned)gxd;
+        *gy = (unsigned)std::max<size_t>(1, std::min<size_t>({nb_x, 65535, kNoAllocMaxBlocks / gxd}));
+    }
+    return *gx * *gy;
 }
 
 } // namespace
@@ -585,8 +654,9 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
         return kErrArg;
     }
     int rc;
-    unsigned char *base = noalloc_scratch(&rc);
-    if (!base) return rc;
+    NoAllocEntry *ent = noalloc_entry("hydro2d_step_f64_noalloc", &rc);
+    if (!ent) return rc;
+    unsigned char *base = ent->base;
     StepScratch *scr = reinterpret_cast<StepScratch *>(base);
     StepStatus *status = reinterpret_cast<StepStatus *>(base + sizeof(StepScratch));
     double2 *partials = reinterpret_cast<double2 *>(base + kNoAllocHeader);
@@ -603,9 +673,10 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
         if (info) *info = hydro_step_info_t{0.0, 0.0, 0u, 0};
         return kOk;
     }
-    // the reduction words must start at zero: clear them (the skip history after them is
-    // kept, a stale one only costs a redo pass)
+    // the reduction words and the status record must start at zero: clear them (the skip
+    // history between them is kept, a stale one only costs a redo pass)
     cudaError_t e = cudaMemsetAsync(scr, 0, offsetof(StepScratch, hist_key), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(StepStatus), st);
     if (e != cudaSuccess) {
         set_error(kErrCuda, "hydro2d_step_f64_noalloc: %s", cudaGetErrorString(e));
         return kErrCuda;
@@ -627,30 +698,28 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
     if (strip_ok)
         strip_ok = encode_tmap_2d(&tmr, tmap_type<T>(), d_rhoE, 2 * (NB_Y + 2), NB_X + 2, rowbytes, 2 * kStripNT, 1) &&
                    encode_tmap_2d(&tmu, tmap_type<T>(), d_uv, 2 * (NB_Y + 2), NB_X + 2, rowbytes, 2 * kStripNT, 1);
-    int kernel;
-    if (strip_ok) {
-        // as step2d, with the chunk grown until the blocks fit the fixed partials
-        const size_t max_chunks = kNoAllocMaxBlocks / nstrips;
-        const int target = 148 * 3 * 8;
-        size_t nchunks = (target + nstrips - 1) / nstrips;
-        size_t chunk = std::min<size_t>(256, std::max<size_t>(16, (NB_X + nchunks - 1) / nchunks));
-        chunk = std::max(chunk, (NB_X + std::min<size_t>(max_chunks, 65535) - 1) / std::min<size_t>(max_chunks, 65535));
-        nchunks = (NB_X + chunk - 1) / chunk;
-        g.chunk = (int)chunk;
-        strip2d<T, true><<<dim3((unsigned)nstrips, (unsigned)nchunks), kStripNT, 0, st>>>(tmr, tmu, g);
-        kernel = (int)Kernel::Strip;
-    } else {
-        const size_t gy = std::max<size_t>(1, std::min<size_t>({NB_X, 65535, kNoAllocMaxBlocks / gx_direct}));
-        g.chunk = 0;
-        direct2d<T><<<dim3((unsigned)gx_direct, (unsigned)gy), kDirectNT, 0, st>>>(g);
-        kernel = (int)Kernel::Direct;
+    int chunk = 0;
+    unsigned gx = 0, gy = 0;
+    if (!noalloc_shape(NB_X, NB_Y, strip_ok, device_sms(), &chunk, &gx, &gy)) {
+        set_error(kErrArg, "hydro2d_step_f64_noalloc: grid %zu x %zu exceeds the fixed scratch", NB_X, NB_Y);
+        return kErrArg;
     }
+    g.chunk = chunk;
+    const int kernel = (int)(strip_ok ? Kernel::Strip : Kernel::Direct);
+    if (strip_ok)
+        strip2d<T, true><<<dim3(gx, gy), kStripNT, 0, st>>>(tmr, tmu, g);
+    else
+        direct2d<T><<<dim3(gx, gy), kDirectNT, 0, st>>>(g);
     // the redo pass returns at once unless the step left Dt_next to it
-    redo2d<T><<<148 * 4, kRedoNT, 0, st>>>(g);
+    redo2d<T><<<(unsigned)device_sms() * 4, kRedoNT, 0, st>>>(g);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(kErrCuda, "hydro2d_step_f64_noalloc launch: %s", cudaGetErrorString(e));
         return kErrCuda;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        ent->last_kernel = kernel;
     }
     if (!sync) {
         if (info) info->kernel = kernel;
@@ -673,4 +742,44 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
         return kErrPhys;
     }
     return kOk;
+}
+
+extern "C" int hydro2d_noalloc_last_info(void *stream, hydro_step_info_t *info)
+{
+    using namespace hydro;
+    if (!info) {
+        set_error(kErrArg, "hydro2d_noalloc_last_info: null info");
+        return kErrArg;
+    }
+    int rc;
+    NoAllocEntry *ent = noalloc_entry("hydro2d_noalloc_last_info", &rc);
+    if (!ent) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    StepStatus s;
+    cudaError_t e = cudaMemcpyAsync(&s, ent->base + sizeof(StepScratch), sizeof s, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "hydro2d_noalloc_last_info: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    int kernel;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        kernel = ent->last_kernel;
+    }
+    *info = hydro_step_info_t{s.mass + s.mass_comp, s.max_speed, s.err, kernel};
+    if (s.err & kErrWaitTimeout) return kErrTimeout;
+    return (s.err & kErrNonPhysical) ? kErrPhys : kOk;
+}
+
+extern "C" unsigned hydro2d_noalloc_launch_shape(size_t NB_X, size_t NB_Y, int strip, int sms, int *chunk,
+                                                 unsigned *grid_x, unsigned *grid_y)
+{
+    int c = 0;
+    unsigned gx = 0, gy = 0;
+    const unsigned n = hydro::noalloc_shape(NB_X, NB_Y, strip != 0, sms, &c, &gx, &gy);
+    if (chunk) *chunk = c;
+    if (grid_x) *grid_x = gx;
+    if (grid_y) *grid_y = gy;
+    return n;
 }

@@ -243,7 +243,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
             set_error(kErrArg, "step3d: NB_Y %zu too large for the strip kernel", nb_y);
             return kErrArg;
         }
-        const int target = 148 * 2 * 8;
+        const int target = device_sms() * 2 * 8;
         int nchunks = std::max(1, (target + nz * ny - 1) / (nz * ny));
         int chunk = (int)((nb_x + nchunks - 1) / nchunks);
         chunk = std::min(256, std::max(8, chunk));
@@ -282,7 +282,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         return kErrCuda;
     }
     ctx->last_kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
-    const unsigned redo_blocks = 148 * 4;
+    const unsigned redo_blocks = (unsigned)device_sms() * 4;
     if (!sync) {
         // enqueued unconditionally; returns at once unless the step asked for it
         redo3d<T><<<redo_blocks, k3RedoNT, 0, stream>>>(g);
@@ -338,7 +338,7 @@ int init3d_at(T *rhoE, T *uvw, size_t nb_x, size_t nb_y, size_t nb_z, double cx,
         const long long zs = (long long)nb_z + 2, zy = (long long)(nb_y + 2) * zs;
         // 16 blocks of 128 threads per SM; each thread takes nb_x / gz planes of its column
         const size_t gxy = ((nb_z + 31) / 32) * ((nb_y + 3) / 4);
-        const size_t gz = std::max<size_t>(1, std::min<size_t>({nb_x, 65535, (size_t)148 * 16 / std::min<size_t>(gxy, 148 * 16)}));
+        const size_t gz = std::max<size_t>(1, std::min<size_t>({nb_x, 65535, (size_t)device_sms() * 16 / std::min<size_t>(gxy, (size_t)device_sms() * 16)}));
         dim3 grid((unsigned)((nb_z + 31) / 32), (unsigned)((nb_y + 3) / 4), (unsigned)gz);
         init3d_kernel<T><<<grid, dim3(32, 4), 0, stream>>>(rhoE, uvw, (int)nb_x, (int)nb_y, (int)nb_z, zs, zy, cx, cy,
                                                            cz, radius, u_in, u_out, p_in, p_out, C_min, gamma, gm1,

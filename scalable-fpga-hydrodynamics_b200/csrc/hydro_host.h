@@ -70,6 +70,11 @@ inline unsigned long long problem_key(const void *dt_next, size_t a, size_t b, s
 
 // Context of the current device (created on first use; never freed before exit).
 DevCtx *ctx_current(int *err);
+// Number of device contexts created so far in this process.
+int ctx_count();
+// Streaming multiprocessors of the current device, queried once per device (launch
+// shapes are sized in multiples of it); 1 if the query fails.
+int device_sms();
 // Grow the partials array to at least n entries (synchronises the device on growth).
 int ctx_reserve(DevCtx *c, size_t n);
 

@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 import re
 import sys
 from pathlib import Path
@@ -35,7 +36,9 @@ sys.modules["hydro_b200"] = pkg
 spec.loader.exec_module(pkg)
 import oracle as orc  # noqa: E402
 
-REF = Path("/root/reference")
+# the reference checkout: HYDRO_REFERENCE_DIR, else a checkout named `reference` beside
+# this repository
+REF = Path(os.environ.get("HYDRO_REFERENCE_DIR") or ROOT.parent / "reference")
 OUT = Path(__file__).resolve().parent
 
 

@@ -16,7 +16,8 @@ HEADER = ROOT / "include" / "hydro_b200.h"
 
 def declared_functions():
     txt = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
-    names = re.findall(r"^\s*(?:const\s+)?(?:double|float|int|void|char)\s*\*?\s*(hydro\w+)\s*\(", txt, flags=re.M)
+    names = re.findall(r"^\s*(?:const\s+)?(?:double|float|int|void|char|unsigned|long long)\s*\*?\s*(hydro\w+)\s*\(",
+                       txt, flags=re.M)
     assert len(names) >= 18
     return sorted(set(names))
 
@@ -50,3 +51,28 @@ def test_queue_struct_layout():
     include/compat/sycl/sycl.hpp (checked there by static_assert)."""
     assert ctypes.sizeof(hb.Queue) == 16
     assert ctypes.sizeof(hb.StepInfo) == 24
+
+
+def test_noalloc_launch_shape_fits_the_fixed_scratch(built):
+    """The allocation-free step's launch shape (host only): at most 65536 blocks, every
+    row covered, and the chunk grown where the default shape would exceed the cap."""
+    fn = built.hydro2d_noalloc_launch_shape
+    fn.argtypes = [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                   ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint)]
+    fn.restype = ctypes.c_uint
+    c, gx, gy = ctypes.c_int(), ctypes.c_uint(), ctypes.c_uint()
+    for nb_x, nb_y, strip in ((60, 60, 1), (100000, 126 * 4096, 1), (40000, 20000, 1), (1 << 20, 126 * 65536, 1),
+                              (3000, 8257536, 1), (100000, 126 * 4096, 0), (70000, 128 * 300, 0), (5, 7, 0)):
+        n = fn(nb_x, nb_y, strip, 148, ctypes.byref(c), ctypes.byref(gx), ctypes.byref(gy))
+        assert 0 < n <= 65536 and n == gx.value * gy.value
+        assert gy.value <= 65535
+        if strip:
+            assert gx.value == -(-nb_y // 126)
+            assert c.value * gy.value >= nb_x > c.value * (gy.value - 1)
+        else:
+            assert gx.value == -(-nb_y // 128) and c.value == 0
+    # the default shape of 100000 x 516096 would need 391 chunks of 256 rows per strip:
+    # 4096 strips leave room for 16, so the chunk grows to 6250 rows
+    fn(100000, 126 * 4096, 1, 148, ctypes.byref(c), ctypes.byref(gx), ctypes.byref(gy))
+    assert (c.value, gy.value) == (6250, 16)
+    assert fn(10, 126 * 65536 + 1, 1, 148, ctypes.byref(c), ctypes.byref(gx), ctypes.byref(gy)) == 0
