@@ -55,6 +55,20 @@ typedef struct hydro_queue {
  * host loop exchanging subdomain edges (hydro2d/main.cxx:349-424, --sdx N). */
 #define HYDRO_X_GHOSTS_FROM_MEMORY 0x100
 
+/* Arithmetic of a step, as bits of hydro_queue_t.flags (launchers) or of the `kernel`
+ * argument (step entry points).
+ * HYDRO_ARITH_STRICT: every operation rounded once, in the reference's order, no
+ *   contraction: bit-identical to the reference kernel compiled with -ffp-contract=off.
+ * HYDRO_ARITH_FUSED: the same formulas with products that feed sums fused (one rounding),
+ *   and reciprocals / square roots from the hardware approximations refined by one
+ *   third-order step; results differ from strict by a few units in the last place per
+ *   operation (not bit-identical), as the reference's own contracting build (-march=native)
+ *   differs from its strict one.
+ * With neither bit the step is strict. STRICT wins if both are set. The direct kernel
+ * (HYDRO_KERNEL_DIRECT, and the fallback for misaligned arrays) is always strict. */
+#define HYDRO_ARITH_FUSED 0x200
+#define HYDRO_ARITH_STRICT 0x400
+
 /* Extra results of one step, beyond what the reference's launcher returns. */
 typedef struct hydro_step_info {
     double mass;      /* compensated FP64 sum of the new interior density */
@@ -296,6 +310,12 @@ int hydro3d_init_blast_at_f64(double *d_rhoE, double *d_uvw, size_t NB_X, size_t
 int hydro3d_init_blast_at_f32(float *d_rhoE, float *d_uvw, size_t NB_X, size_t NB_Y, size_t NB_Z, double cx,
                               double cy, double cz, double radius, float rho_in, float rho_out, float p_in,
                               float p_out, float C_min, float gamma, float *min_dt, void *stream);
+
+/* Diagnostics: the reciprocal and square root of n device values as the fused arithmetic
+ * (HYDRO_ARITH_FUSED) computes them, for comparison with the correctly rounded values.
+ * Synchronous. No counterpart in the reference. */
+int hydro_fused_math_f64(const double *d_x, size_t n, double *d_rcp, double *d_sqrt, void *stream);
+int hydro_fused_math_f32(const float *d_x, size_t n, float *d_rcp, float *d_sqrt, void *stream);
 
 /* ---- errors -------------------------------------------------------------------------- */
 /* No counterpart in the reference (it has no status return): last error code latched

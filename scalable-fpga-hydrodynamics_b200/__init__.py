@@ -27,6 +27,10 @@ KERNEL_AUTO, KERNEL_STRIP, KERNEL_DIRECT = 0, 1, 2
 # X neighbours of the first and last interior rows (planes) from the input's ghost rows
 # instead of the in-kernel periodic wrap (include/hydro_b200.h)
 X_GHOSTS_FROM_MEMORY = 0x100
+# arithmetic of a step (include/hydro_b200.h): strict (the reference's order, bit-identical)
+# or fused (fma contraction, refined hardware reciprocal / square root)
+ARITH_FUSED, ARITH_STRICT = 0x200, 0x400
+_ARITH_BITS = {None: 0, "strict": ARITH_STRICT, "fused": ARITH_FUSED}
 HYDRO_OK, HYDRO_ERR_ARG, HYDRO_ERR_CUDA, HYDRO_ERR_NONPHYSICAL, HYDRO_ERR_TIMEOUT = 0, -1, -2, -3, -4
 
 _c_size = ctypes.c_size_t
@@ -190,37 +194,39 @@ class Physics:
 
 # ----------------------------------------------------------------------- drop-in ABI ---
 def launcher2d(rhoE, uv, rhoE_next, uv_next, dt_next, C_min, gamma, gm1, divgamma, K, nb_x, nb_y, DtDx, DtDy,
-               stream=None, device=-1):
+               stream=None, device=-1, arith=None):
     """The reference launcher signature (hydro2d/kernel.hpp:63-68) over torch tensors;
     returns the elapsed microseconds like the reference (negative on error)."""
     L = lib()
     f64 = rhoE.dtype.itemsize == 8
     T, fn = (ctypes.c_double, L.hydro2d_launcher_f64) if f64 else (ctypes.c_float, L.hydro2d_launcher_f32)
     dx, dy = T(DtDx), T(DtDy)
-    q = Queue(_stream_handle(stream), device, 0)
+    q = Queue(_stream_handle(stream), device, _ARITH_BITS[arith])
     return fn(_ptr(rhoE), _ptr(uv), _ptr(rhoE_next), _ptr(uv_next), _ptr(dt_next), C_min, gamma, gm1, divgamma, K,
               nb_x, nb_y, ctypes.byref(dx), ctypes.byref(dy), q)
 
 
 def launcher3d(rhoE, uvw, rhoE_next, uvw_next, dt_next, C_min, gamma, gm1, divgamma, K, nb_x, nb_y, nb_z, DtDx,
-               DtDy, DtDz, stream=None, device=-1):
+               DtDy, DtDz, stream=None, device=-1, arith=None):
     """The reference launcher signature (hydro3d/kernel.hpp:64-69) over torch tensors."""
     L = lib()
     f64 = rhoE.dtype.itemsize == 8
     T, fn = (ctypes.c_double, L.hydro3d_launcher_f64) if f64 else (ctypes.c_float, L.hydro3d_launcher_f32)
     dx, dy, dz = T(DtDx), T(DtDy), T(DtDz)
-    q = Queue(_stream_handle(stream), device, 0)
+    q = Queue(_stream_handle(stream), device, _ARITH_BITS[arith])
     return fn(_ptr(rhoE), _ptr(uvw), _ptr(rhoE_next), _ptr(uvw_next), _ptr(dt_next), C_min, gamma, gm1, divgamma,
               K, nb_x, nb_y, nb_z, ctypes.byref(dx), ctypes.byref(dy), ctypes.byref(dz), q)
 
 
 def step(state_in, state_out, dt_next, phys: Physics, dtd, kernel=KERNEL_AUTO, sync=True, stream=None,
-         check=True, x_ghosts=False):
+         check=True, x_ghosts=False, arith=None):
     """One step through hydro{2d,3d}_step_{f64,f32}. state_* = (rhoE, uvx) tensors.
-    x_ghosts: read the X ghost rows (planes) of state_in instead of wrapping periodically."""
+    x_ghosts: read the X ghost rows (planes) of state_in instead of wrapping periodically.
+    arith: "strict", "fused" or None (the library default)."""
     L = lib()
     if x_ghosts:
         kernel |= X_GHOSTS_FROM_MEMORY
+    kernel |= _ARITH_BITS[arith]
     f64 = phys.dtype is np.float64
     suf = "f64" if f64 else "f32"
     info = StepInfo()
@@ -334,12 +340,14 @@ class BlastRun:
     (hydro2d/main.cxx:686-815): state stays on the device; each step reads the new Dt
     back (the only per-step device-to-host copy the loop needs)."""
 
-    def __init__(self, nb, dtype=np.float64, kernel=KERNEL_AUTO, stream=None, blast=None):
+    def __init__(self, nb, dtype=np.float64, kernel=KERNEL_AUTO, stream=None, blast=None, arith=None):
         """`blast` (a hydro_b200.batch.Blast) overrides the reference's initial condition
-        and constants with an explicit centre, radius, densities, pressures, gamma, K, C."""
+        and constants with an explicit centre, radius, densities, pressures, gamma, K, C.
+        `arith`: "strict", "fused" or None (the library default)."""
         torch = _torch()
         self.nb = tuple(int(n) for n in nb)
         self.T = dtype
+        self.arith = arith
         if blast is None:
             self.phys = Physics(dtype, self.nb)
         else:
@@ -367,7 +375,8 @@ class BlastRun:
     def step_kernel_only(self):
         """Enqueue this step's kernel on the stream without waiting."""
         dtd = self.phys.dtd(self.dt)
-        step(self.cur, self.nxt, self.dt_dev, self.phys, dtd, kernel=self.kernel, sync=False, stream=self.stream)
+        step(self.cur, self.nxt, self.dt_dev, self.phys, dtd, kernel=self.kernel, sync=False, stream=self.stream,
+             arith=self.arith)
 
     def step_finish(self):
         """Wait for the step, check its status, swap buffers and read the new Dt back."""

@@ -1,4 +1,5 @@
 // extern "C" entry points declared in include/hydro_b200.h.
+#include <algorithm>
 #include <stdio.h>
 #include <time.h>
 
@@ -48,7 +49,14 @@ double finish_launcher(int rc, double t0, const char *what)
 
 template <class T> Phys<T> phys(T C_min, T gamma, T gm1, T divgamma, T K)
 {
-    return Phys<T>{C_min, gamma, gm1, divgamma, K, K < T(0)};
+    return Phys<T>::make(C_min, gamma, gm1, divgamma, K);
+}
+
+// The arithmetic a step runs in, from the HYDRO_ARITH_* bits of the flags.
+bool fused_of(int flags)
+{
+    if (flags & HYDRO_ARITH_STRICT) return false;
+    return (flags & HYDRO_ARITH_FUSED) != 0;
 }
 
 void fill(hydro_step_info_t *out, const StepInfo &in)
@@ -60,9 +68,47 @@ void fill(hydro_step_info_t *out, const StepInfo &in)
     out->kernel = in.kernel;
 }
 
+// Fused-mode reciprocal and square root of each value (diagnostics: the tests compare them
+// with the correctly rounded values).
+template <class T> __global__ void fused_math_kernel(const T *x, long long n, T *rcp, T *sq)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        rcp[i] = Fu<T>::rcp(x[i]);
+        sq[i] = Fu<T>::sqrt(x[i]);
+    }
+}
+
+template <class T> int fused_math(const T *x, size_t n, T *rcp, T *sq, void *stream)
+{
+    if (!x || !rcp || !sq) {
+        set_error(kErrArg, "hydro_fused_math: null argument");
+        return kErrArg;
+    }
+    if (n == 0) return kOk;
+    const cudaStream_t st = (cudaStream_t)stream;
+    const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)device_sms() * 8);
+    fused_math_kernel<T><<<blocks, 256, 0, st>>>(x, (long long)n, rcp, sq);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        set_error(kErrCuda, "hydro_fused_math: %s", cudaGetErrorString(e));
+        return kErrCuda;
+    }
+    return kOk;
+}
+
 } // namespace
 
 extern "C" {
+
+int hydro_fused_math_f64(const double *d_x, size_t n, double *d_rcp, double *d_sqrt, void *stream)
+{
+    return fused_math<double>(d_x, n, d_rcp, d_sqrt, stream);
+}
+int hydro_fused_math_f32(const float *d_x, size_t n, float *d_rcp, float *d_sqrt, void *stream)
+{
+    return fused_math<float>(d_x, n, d_rcp, d_sqrt, stream);
+}
 
 double hydro2d_launcher_f64(const double *d_rhoE, const double *d_uv, double *d_rhoE_next, double *d_uv_next,
                             double *Dt_next, double C_min, double gamma, double gamma_minus_one, double divgamma,
@@ -79,7 +125,7 @@ double hydro2d_launcher_f64(const double *d_rhoE, const double *d_uv, double *d_
     const int rc = step2d<double>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
                                   phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, *DtDx, *DtDy,
                                   (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr,
-                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
+                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0, fused_of(queue.flags));
     return finish_launcher(rc, t0, "launcher");
 }
 
@@ -97,7 +143,7 @@ double hydro2d_launcher_f32(const float *d_rhoE, const float *d_uv, float *d_rho
     const int rc = step2d<float>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, *DtDx, *DtDy,
                                  (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr,
-                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
+                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0, fused_of(queue.flags));
     return finish_launcher(rc, t0, "launcher");
 }
 
@@ -116,7 +162,7 @@ double hydro3d_launcher_f64(const double *d_rhoE, const double *d_uvw, double *d
     const int rc = step3d<double>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
                                   phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, *DtDx, *DtDy,
                                   *DtDz, (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr,
-                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
+                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0, fused_of(queue.flags));
     return finish_launcher(rc, t0, "launcher");
 }
 
@@ -135,7 +181,7 @@ double hydro3d_launcher_f32(const float *d_rhoE, const float *d_uvw, float *d_rh
     const int rc = step3d<float>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, *DtDx, *DtDy,
                                  *DtDz, (cudaStream_t)queue.stream, Kernel::Auto, true, nullptr,
-                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
+                                  (queue.flags & HYDRO_X_GHOSTS_FROM_MEMORY) == 0, fused_of(queue.flags));
     return finish_launcher(rc, t0, "launcher");
 }
 
@@ -148,7 +194,7 @@ int hydro2d_step_f64(const double *d_rhoE, const double *d_uv, double *d_rhoE_ne
     const int rc = step2d<double>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
                                   phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, DtDx, DtDy,
                                   (cudaStream_t)stream, (Kernel)(kernel & 0xff), sync != 0, &si,
-                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
+                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0, fused_of(kernel));
     fill(info, si);
     return rc;
 }
@@ -162,7 +208,7 @@ int hydro2d_step_f32(const float *d_rhoE, const float *d_uv, float *d_rhoE_next,
     const int rc = step2d<float>(d_rhoE, d_uv, d_rhoE_next, d_uv_next, Dt_next,
                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, DtDx, DtDy,
                                  (cudaStream_t)stream, (Kernel)(kernel & 0xff), sync != 0, &si,
-                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
+                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0, fused_of(kernel));
     fill(info, si);
     return rc;
 }
@@ -176,7 +222,7 @@ int hydro3d_step_f64(const double *d_rhoE, const double *d_uvw, double *d_rhoE_n
     const int rc = step3d<double>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
                                   phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, DtDx, DtDy,
                                   DtDz, (cudaStream_t)stream, (Kernel)(kernel & 0xff), sync != 0, &si,
-                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
+                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0, fused_of(kernel));
     fill(info, si);
     return rc;
 }
@@ -190,7 +236,7 @@ int hydro3d_step_f32(const float *d_rhoE, const float *d_uvw, float *d_rhoE_next
     const int rc = step3d<float>(d_rhoE, d_uvw, d_rhoE_next, d_uvw_next, Dt_next,
                                  phys(C_min, gamma, gamma_minus_one, divgamma, K), NB_X, NB_Y, NB_Z, DtDx, DtDy, DtDz,
                                  (cudaStream_t)stream, (Kernel)(kernel & 0xff), sync != 0, &si,
-                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0);
+                                  (kernel & HYDRO_X_GHOSTS_FROM_MEMORY) == 0, fused_of(kernel));
     fill(info, si);
     return rc;
 }

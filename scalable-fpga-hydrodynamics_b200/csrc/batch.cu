@@ -644,12 +644,10 @@ template <class T, int D> class BatchEngine final : public BatchBase {
             I.DZ = one / T(nb_z + 1);
             ms = (I.DZ < ms) ? I.DZ : ms;
         }
-        I.ph.C_min = T(T(s.C) * ms);
-        I.ph.gamma = T(s.gamma);
-        I.ph.gm1 = T(I.ph.gamma - one);
-        I.ph.divgamma = T(one / I.ph.gm1);
-        I.ph.K = T(s.K);
-        I.ph.kneg = I.ph.K < T(0);
+        {
+            const T gamma = T(s.gamma), gm1 = T(gamma - one);
+            I.ph = Phys<T>::make(T(T(s.C) * ms), gamma, gm1, T(one / gm1), T(s.K));
+        }
         I.ggm1 = skip_ggm1(I.ph.gamma, I.ph.gm1);
         T first = 0;
         int rc;

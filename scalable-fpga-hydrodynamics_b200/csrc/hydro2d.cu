@@ -102,21 +102,23 @@ template <class T> __global__ void __launch_bounds__(kDirectNT) direct2d(Args2<T
 // Redo pass: the exact signal speed of every interior cell of the new state, when the
 // step's skip threshold turned out too high (StepScratch::redo); exits at once otherwise.
 constexpr int kRedoNT = 256;
-template <class T> __global__ void __launch_bounds__(kRedoNT) redo2d(Args2<T> g)
+template <class T, bool kF = false> __global__ void __launch_bounds__(kRedoNT) redo2d(Args2<T> g)
 {
     if (*reinterpret_cast<const volatile unsigned *>(&g.scr->redo) == 0u) return;
     StepAcc acc;
     const long long n = (long long)g.nb_x * g.nb_y;
     for (long long q = blockIdx.x * (long long)kRedoNT + threadIdx.x; q < n; q += (long long)gridDim.x * kRedoNT) {
         const long long c = (1 + q / g.nb_y) * g.ys + 1 + q % g.nb_y;
-        acc.add_speed(speed2(g.rhoE_n[2 * c], g.uv_n[2 * c], g.uv_n[2 * c + 1], g.rhoE_n[2 * c + 1], g.ph));
+        acc.add_speed(
+            speed2<T, kF>(g.rhoE_n[2 * c], g.uv_n[2 * c], g.uv_n[2 * c + 1], g.rhoE_n[2 * c + 1], g.ph));
     }
     redo_epilogue<kRedoNT, T>(acc.vmax, acc.err, g.scr, gridDim.x, g.ph.C_min, g.Dt_next, g.status, g.key);
 }
 
 // ------------------------------------------------------------------- strip kernel ---
 // kTma: rows staged by TMA tile loads (16-byte row pitch), else by per-lane cp.async.
-template <class T, bool kTma>
+// kF: fused arithmetic (hydro_math.cuh).
+template <class T, bool kTma, bool kF>
 __global__ void __launch_bounds__(kStripNT, 4)
     strip2d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args2<T> g)
 {
@@ -134,12 +136,13 @@ __global__ void __launch_bounds__(kStripNT, 4)
     const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
     const Phys<T> ph = g.ph;
     unsigned ld = 0;
-    const bool ok = march2d<T, kTma>(S, &tmr, &tmu, geo, g.rhoE_n, g.uv_n, ph, g.DtDx, g.DtDy, ld, [&](const Upd2<T> &o) {
-        acc.add_mass(o.r);
-        const float fu = (float)o.u, fv = (float)o.v;
-        if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1, tlo2))
-            acc.add_speed(speed2(o.r, o.u, o.v, o.E, ph));
-    });
+    const bool ok = march2d<T, kTma, kF>(S, &tmr, &tmu, geo, g.rhoE_n, g.uv_n, ph, g.DtDx, g.DtDy, ld,
+                                         [&](const Upd2<T> &o) {
+                                             acc.add_mass(o.r);
+                                             const float fu = (float)o.u, fv = (float)o.v;
+                                             if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1, tlo2))
+                                                 acc.add_speed(speed2<T, kF>(o.r, o.u, o.v, o.E, ph));
+                                         });
     if (!ok) acc.err |= kErrWaitTimeout;
     step_epilogue<kStripNT, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y, blockIdx.x + blockIdx.y * gridDim.x,
                                g.ph.C_min, g.Dt_next, g.status, g.seq, (double)tlof, g.key);
@@ -284,7 +287,8 @@ bool aligned(const void *p, size_t a) { return (reinterpret_cast<uintptr_t>(p) %
 
 template <class T>
 int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
-           size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info, bool xwrap)
+           size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info, bool xwrap,
+           bool fused)
 {
     if (!rhoE || !uv || !rhoE_next || !uv_next || !Dt_next) {
         set_error(kErrArg, "step2d: null pointer argument");
@@ -361,10 +365,15 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
         nblocks = (unsigned)nstrips * (unsigned)nchunks;
         if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
         g.partials = ctx->partials;
-        if (tma_ok)
-            strip2d<T, true><<<dim3(nstrips, nchunks), kStripNT, 0, stream>>>(tmr, tmu, g);
+        const dim3 grid(nstrips, nchunks);
+        if (tma_ok && fused)
+            strip2d<T, true, true><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
+        else if (tma_ok)
+            strip2d<T, true, false><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
+        else if (fused)
+            strip2d<T, false, true><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
         else
-            strip2d<T, false><<<dim3(nstrips, nchunks), kStripNT, 0, stream>>>(tmr, tmu, g);
+            strip2d<T, false, false><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
     } else {
         const int gx = (int)((nb_y + kDirectNT - 1) / kDirectNT);
         const int gy = (int)std::min<size_t>(nb_x, 65535);
@@ -382,9 +391,18 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
     }
     ctx->last_kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
     const unsigned redo_blocks = (unsigned)device_sms() * 4;
+    // the redo pass recomputes the signal speed in the arithmetic of the step that ran
+    // (the direct kernel is always strict)
+    const bool fused_ran = fused && use_strip;
+    auto redo = [&]() {
+        if (fused_ran)
+            redo2d<T, true><<<redo_blocks, kRedoNT, 0, stream>>>(g);
+        else
+            redo2d<T, false><<<redo_blocks, kRedoNT, 0, stream>>>(g);
+    };
     if (!sync) {
         // enqueued unconditionally; returns at once unless the step asked for it
-        redo2d<T><<<redo_blocks, kRedoNT, 0, stream>>>(g);
+        redo();
         e = cudaGetLastError();
         if (e != cudaSuccess) {
             ctx->dirty = true;
@@ -396,7 +414,7 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
     }
     e = cudaStreamSynchronize(stream);
     if (e == cudaSuccess && read_status(ctx->status_h).redo) {
-        redo2d<T><<<redo_blocks, kRedoNT, 0, stream>>>(g);
+        redo();
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     }
@@ -501,9 +519,9 @@ template <class T> int mass_sum(const T *rhoE, size_t nb_x, size_t nb_y, size_t 
 }
 
 template int step2d<double>(const double *, const double *, double *, double *, double *, const Phys<double> &,
-                            size_t, size_t, double, double, cudaStream_t, Kernel, bool, StepInfo *, bool);
+                            size_t, size_t, double, double, cudaStream_t, Kernel, bool, StepInfo *, bool, bool);
 template int step2d<float>(const float *, const float *, float *, float *, float *, const Phys<float> &, size_t,
-                           size_t, float, float, cudaStream_t, Kernel, bool, StepInfo *, bool);
+                           size_t, float, float, cudaStream_t, Kernel, bool, StepInfo *, bool, bool);
 template int init2d<double>(double *, double *, size_t, size_t, double, double, double, double, double, double,
                             double *, cudaStream_t);
 template int init2d_at<double>(double *, double *, size_t, size_t, double, double, double, double, double, double,
@@ -661,7 +679,7 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
     StepStatus *status = reinterpret_cast<StepStatus *>(base + sizeof(StepScratch));
     double2 *partials = reinterpret_cast<double2 *>(base + kNoAllocHeader);
 
-    const Phys<T> ph{C_min, gamma, gamma_minus_one, divgamma, K, K < 0.0};
+    const Phys<T> ph = Phys<T>::make(C_min, gamma, gamma_minus_one, divgamma, K);
     if (NB_X == 0 || NB_Y == 0) {
         const T dt = div_zero(C_min);
         cudaError_t e = cudaMemcpyAsync(Dt_next, &dt, sizeof(T), cudaMemcpyHostToDevice, st);
@@ -707,7 +725,7 @@ extern "C" int hydro2d_step_f64_noalloc(const double *d_rhoE, const double *d_uv
     g.chunk = chunk;
     const int kernel = (int)(strip_ok ? Kernel::Strip : Kernel::Direct);
     if (strip_ok)
-        strip2d<T, true><<<dim3(gx, gy), kStripNT, 0, st>>>(tmr, tmu, g);
+        strip2d<T, true, false><<<dim3(gx, gy), kStripNT, 0, st>>>(tmr, tmu, g);
     else
         direct2d<T><<<dim3(gx, gy), kDirectNT, 0, st>>>(g);
     // the redo pass returns at once unless the step left Dt_next to it

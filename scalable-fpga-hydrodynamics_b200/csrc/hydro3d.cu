@@ -18,6 +18,7 @@
 //  direct3d  one thread per cell, the 7-point stencil loaded directly, every face
 //            evaluated from both sides like the reference.
 #include <algorithm>
+#include <cstring>
 #include <stdio.h>
 
 #include "hydro_host.h"
@@ -90,7 +91,7 @@ template <class T> __global__ void __launch_bounds__(128) direct3d(Args3<T> g)
 
 // Redo pass (see StepScratch): the exact signal speed of every interior cell.
 constexpr int k3RedoNT = 256;
-template <class T> __global__ void __launch_bounds__(k3RedoNT) redo3d(Args3<T> g)
+template <class T, bool kF = false> __global__ void __launch_bounds__(k3RedoNT) redo3d(Args3<T> g)
 {
     if (*reinterpret_cast<const volatile unsigned *>(&g.scr->redo) == 0u) return;
     StepAcc acc;
@@ -99,17 +100,28 @@ template <class T> __global__ void __launch_bounds__(k3RedoNT) redo3d(Args3<T> g
     for (long long q = blockIdx.x * (long long)k3RedoNT + threadIdx.x; q < n; q += (long long)gridDim.x * k3RedoNT) {
         const long long r = q % ncol;
         const long long c = (1 + q / ncol) * g.zy + (1 + r / g.nb_z) * g.zs + 1 + r % g.nb_z;
-        acc.add_speed(speed3(g.rhoE_n[2 * c], g.uvw_n[3 * c], g.uvw_n[3 * c + 1], g.uvw_n[3 * c + 2],
-                             g.rhoE_n[2 * c + 1], g.ph));
+        acc.add_speed(speed3<T, kF>(g.rhoE_n[2 * c], g.uvw_n[3 * c], g.uvw_n[3 * c + 1], g.uvw_n[3 * c + 2],
+                                    g.rhoE_n[2 * c + 1], g.ph));
     }
     redo_epilogue<k3RedoNT, T>(acc.vmax, acc.err, g.scr, gridDim.x, g.ph.C_min, g.Dt_next, g.status, g.key);
 }
 
 // ------------------------------------------------------------------- strip kernel ---
-template <class T> __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) strip3d(Args3<T> g)
+// kF: fused arithmetic (hydro_math.cuh). kTma: planes staged by the tensor maps tmr/tmu
+// (FP64, even NB_Z), else by per-lane cp.async.
+template <class T, bool kF, bool kTma>
+__global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>)
+    strip3d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args3<T> g)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     Smem3<T> &S = *reinterpret_cast<Smem3<T> *>(smem_raw);
+    if constexpr (kTma) {
+        if (threadIdx.x == 0) {
+            prefetch_tensormap(&tmr);
+            prefetch_tensormap(&tmu);
+        }
+        march3d_init(S);
+    }
     const int i0 = 1 + g.chunk * (int)blockIdx.z;
     const March3 geo{k3TZ * (int)blockIdx.x, k3TY<T> * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
                      g.nb_x, g.nb_y, g.nb_z, g.zs, g.zy, g.xwrap};
@@ -117,12 +129,16 @@ template <class T> __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) st
     const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
     const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
     const Phys<T> ph = g.ph;
-    march3d<T>(S, g.rhoE, g.uvw, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz, [&](const Upd3<T> &o) {
-        acc.add_mass(o.r);
-        const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
-        if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1, tlo2))
-            acc.add_speed(speed3(o.r, o.u, o.v, o.w, o.E, ph));
-    });
+    const bool ok = march3d<T, kF, kTma>(
+        S, g.rhoE, g.uvw, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz,
+        [&](const Upd3<T> &o) {
+            acc.add_mass(o.r);
+            const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
+            if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1, tlo2))
+                acc.add_speed(speed3<T, kF>(o.r, o.u, o.v, o.w, o.E, ph));
+        },
+        Tmaps3{&tmr, &tmu});
+    if (!ok) acc.err |= kErrWaitTimeout;
     step_epilogue<k3NT<T>, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
                            blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
                            g.status, g.seq, (double)tlof, g.key);
@@ -193,10 +209,17 @@ __global__ void init3d_kernel(T *rhoE, T *uvw, int nb_x, int nb_y, int nb_z, lon
 }
 
 // ----------------------------------------------------------------- host drivers ---
+namespace {
+template <class T> CUtensorMapDataType tmap_type3();
+template <> CUtensorMapDataType tmap_type3<double>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT64; }
+template <> CUtensorMapDataType tmap_type3<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) % 16) == 0; }
+} // namespace
+
 template <class T>
 int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
            size_t nb_y, size_t nb_z, T DtDx, T DtDy, T DtDz, cudaStream_t stream, Kernel which, bool sync,
-           StepInfo *info, bool xwrap)
+           StepInfo *info, bool xwrap, bool fused)
 {
     if (!rhoE || !uvw || !rhoE_next || !uvw_next || !Dt_next) {
         set_error(kErrArg, "step3d: null pointer argument");
@@ -256,13 +279,29 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         nblocks = (unsigned)nz * ny * nchunks;
         if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
         g.partials = ctx->partials;
+        // planes by tensor maps where the rows of both arrays are 16-byte pitched (FP64
+        // with even NB_Z; the tile's kbase is a multiple of 30, so even) and the arrays
+        // 16-byte aligned; by per-lane copies otherwise
+        CUtensorMap tmr, tmu;
+        std::memset(&tmr, 0, sizeof tmr);
+        std::memset(&tmu, 0, sizeof tmu);
+        bool tma = sizeof(T) == 8 && (nb_z + 2) % 2 == 0 && aligned16(rhoE) && aligned16(uvw);
+        if (tma) {
+            const uint64_t zs = nb_z + 2, ys = nb_y + 2, xs = nb_x + 2;
+            tma = encode_tmap_3d(&tmr, tmap_type3<T>(), rhoE, 2 * zs, ys, xs, 2 * zs * sizeof(T), 2 * zs * ys * sizeof(T),
+                                 64, k3Warps<T>, 1) &&
+                  encode_tmap_3d(&tmu, tmap_type3<T>(), uvw, 3 * zs, ys, xs, 3 * zs * sizeof(T), 3 * zs * ys * sizeof(T),
+                                 96, k3Warps<T>, 1);
+        }
+        auto kern = fused ? (tma ? strip3d<T, true, true> : strip3d<T, true, false>)
+                          : (tma ? strip3d<T, false, true> : strip3d<T, false, false>);
         const int smem = (int)sizeof(Smem3<T>);
-        cudaError_t ea = cudaFuncSetAttribute(strip3d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (ea != cudaSuccess) {
             set_error(kErrCuda, "step3d: shared-memory attribute: %s", cudaGetErrorString(ea));
             return kErrCuda;
         }
-        strip3d<T><<<dim3(nz, ny, nchunks), k3NT<T>, smem, stream>>>(g);
+        kern<<<dim3(nz, ny, nchunks), k3NT<T>, smem, stream>>>(tmr, tmu, g);
     } else {
         const int gx = (int)((nb_z + 31) / 32), gy = (int)((nb_y + 3) / 4), gz = (int)std::min<size_t>(nb_x, 65535);
         if (gy > 65535) {
@@ -283,9 +322,18 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
     }
     ctx->last_kernel = (int)(use_strip ? Kernel::Strip : Kernel::Direct);
     const unsigned redo_blocks = (unsigned)device_sms() * 4;
+    // the redo pass recomputes the signal speed in the arithmetic of the step that ran
+    // (the direct kernel is always strict)
+    const bool fused_ran = fused && use_strip;
+    auto redo = [&]() {
+        if (fused_ran)
+            redo3d<T, true><<<redo_blocks, k3RedoNT, 0, stream>>>(g);
+        else
+            redo3d<T, false><<<redo_blocks, k3RedoNT, 0, stream>>>(g);
+    };
     if (!sync) {
         // enqueued unconditionally; returns at once unless the step asked for it
-        redo3d<T><<<redo_blocks, k3RedoNT, 0, stream>>>(g);
+        redo();
         e = cudaGetLastError();
         if (e != cudaSuccess) {
             ctx->dirty = true;
@@ -297,7 +345,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
     }
     e = cudaStreamSynchronize(stream);
     if (e == cudaSuccess && read_status(ctx->status_h).redo) {
-        redo3d<T><<<redo_blocks, k3RedoNT, 0, stream>>>(g);
+        redo();
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     }
@@ -379,9 +427,9 @@ template int init3d_at<float>(float *, float *, size_t, size_t, size_t, double, 
 
 template int step3d<double>(const double *, const double *, double *, double *, double *, const Phys<double> &,
                             size_t, size_t, size_t, double, double, double, cudaStream_t, Kernel, bool, StepInfo *,
-                            bool);
+                            bool, bool);
 template int step3d<float>(const float *, const float *, float *, float *, float *, const Phys<float> &, size_t,
-                           size_t, size_t, float, float, float, cudaStream_t, Kernel, bool, StepInfo *, bool);
+                           size_t, size_t, float, float, float, cudaStream_t, Kernel, bool, StepInfo *, bool, bool);
 template int init3d<double>(double *, double *, size_t, size_t, size_t, double, double, double, double, double,
                             double, double *, cudaStream_t);
 template int init3d<float>(float *, float *, size_t, size_t, size_t, float, float, float, float, float, float,

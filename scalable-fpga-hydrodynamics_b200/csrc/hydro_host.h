@@ -114,15 +114,17 @@ struct StepInfo {
 // X neighbours of the first and last interior rows (planes) by periodic wrap inside the
 // kernel (the whole domain on one device); false: from the ghost rows 0 and NB_X+1 of the
 // input, filled by the caller (a subdomain of a multi-rank run).
+// fused: the strip kernels in fused arithmetic (hydro_math.cuh); the direct kernel is
+// always strict.
 template <class T>
 int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
            size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info,
-           bool xwrap = true);
+           bool xwrap = true, bool fused = false);
 
 template <class T>
 int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
            size_t nb_y, size_t nb_z, T DtDx, T DtDy, T DtDz, cudaStream_t stream, Kernel which, bool sync,
-           StepInfo *info, bool xwrap = true);
+           StepInfo *info, bool xwrap = true, bool fused = false);
 
 // Blast initial condition and first Dt on the device (hydro2d/main.cxx:280-338).
 template <class T>

@@ -12,6 +12,15 @@
 // evaluations there take identical arguments, so one evaluation gives the same bits.
 // Quantities that depend on one cell only (primitives, the acoustic impedance
 // sqrt(gamma*p*rho), the upwinded conservative values) are computed once per cell.
+//
+// Every per-cell function takes a template flag kF selecting the arithmetic:
+//  kF = false (strict): the reference's operation order with one rounding per operation,
+//    bit-identical to the reference kernel compiled without contraction;
+//  kF = true (fused): the same formulas with each product that feeds a sum fused into one
+//    rounding (fma), the reciprocal and square roots from the hardware approximations
+//    refined by one third-order step (Fu below), and the energy of z faces taken from the
+//    same sum of squares as x and y faces. Each result differs from the strict one by a few
+//    units in the last place; not bit-identical.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -42,6 +51,76 @@ template <> struct Ar<float> {
     static constexpr float half = 0.5f;
 };
 
+// Fused-mode primitives. Reciprocal and reciprocal square root start from the hardware
+// approximations (PTX rcp.approx.ftz / rsqrt.approx.ftz) and take one third-order
+// Householder step, which cubes the relative error of the start value:
+//   1/a:       e = 1 - a y,          y' = y (1 + e + e^2)
+//   1/sqrt(s): e = 1 - s y^2,        y' = y (1 + e/2 + 3 e^2 / 8)
+// (the truncated binomial series of (1 - e)^-1 and (1 - e)^-1/2). The result is within a
+// few ulp of the correctly rounded value. Inputs outside [2^-1000, 2^1000] (zero,
+// subnormal, huge, negative, NaN), where the flush-to-zero approximations do not apply,
+// take the correctly rounded intrinsic instead.
+template <class T> struct Fu;
+
+template <> struct Fu<double> {
+    static __device__ __forceinline__ bool regular(double a)
+    {
+        const double m = fabs(a);
+        return m >= 0x1p-1000 && m <= 0x1p1000;
+    }
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    static __device__ __forceinline__ double rcp(double a)
+    {
+        if (!regular(a)) return __drcp_rn(a);
+        double y;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+        const double e = __fma_rn(-a, y, 1.0);
+        return __fma_rn(y, __fma_rn(e, e, e), y);
+    }
+    // 1/sqrt(s) for regular s > 0
+    static __device__ __forceinline__ double rsqrt_pos(double s)
+    {
+        double y;
+        asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(s));
+        const double e = __fma_rn(-__dmul_rn(s, y), y, 1.0);
+        return __fma_rn(y, __dmul_rn(e, __fma_rn(0.375, e, 0.5)), y);
+    }
+    static __device__ __forceinline__ double sqrt(double s)
+    {
+        if (!(s > 0.0 && regular(s))) return __dsqrt_rn(s);
+        return __dmul_rn(s, rsqrt_pos(s));
+    }
+};
+
+template <> struct Fu<float> {
+    static __device__ __forceinline__ bool regular(float a)
+    {
+        const float m = fabsf(a);
+        return m >= 0x1p-100f && m <= 0x1p100f;
+    }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    static __device__ __forceinline__ float rcp(float a)
+    {
+        if (!regular(a)) return __frcp_rn(a);
+        float y;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+        const float e = __fmaf_rn(-a, y, 1.0f);
+        return __fmaf_rn(y, __fmaf_rn(e, e, e), y);
+    }
+    static __device__ __forceinline__ float rsqrt_pos(float s)
+    {
+        float y;
+        asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(s));
+        const float e = __fmaf_rn(-__fmul_rn(s, y), y, 1.0f);
+        return __fmaf_rn(y, __fmul_rn(e, __fmaf_rn(0.375f, e, 0.5f)), y);
+    }
+    static __device__ __forceinline__ float sqrt(float s)
+    {
+        if (!(s > 0.0f && regular(s))) return __fsqrt_rn(s);
+        return __fmul_rn(s, rsqrt_pos(s));
+    }
+};
+
 template <class T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
@@ -53,6 +132,12 @@ template <class T> __device__ __forceinline__ T smax(T a, T b) { return (a < b) 
 template <class T> struct Phys {
     T C_min, gamma, gm1, divgamma, K;
     bool kneg; // K < 0
+    T iK;      // 1 / K (fused arithmetic: 1/(K a) = (1/K)(1/a))
+
+    static Phys make(T C_min, T gamma, T gm1, T divgamma, T K)
+    {
+        return Phys{C_min, gamma, gm1, divgamma, K, K < T(0), T(1) / K};
+    }
 };
 
 // A cell seen by the face flux: everything compute_fluxes needs from one side
@@ -90,11 +175,33 @@ template <class T> struct Cell2 {
     T r, u, v, p, Ka, iKa, mu, mv, eup;
 };
 
-template <class T>
+template <class T, bool kF = false>
 __device__ __forceinline__ Cell2<T> make_cell2(T ur, T uu, T uv, T uE, const Phys<T> &ph)
 {
     using A = Ar<T>;
     Cell2<T> c;
+    if constexpr (kF) {
+        using F = Fu<T>;
+        const T inv = F::rcp(ur);
+        c.r = ur;
+        c.u = A::mul(uu, inv);
+        c.v = A::mul(uv, inv);
+        const T temp = F::fma(c.v, c.v, A::mul(c.u, c.u));
+        c.p = A::mul(A::mul(ph.gm1, ur), F::fma(-A::half, temp, A::mul(uE, inv)));
+        const T s = A::mul(A::mul(ph.gamma, c.p), c.r);
+        if (s > T(0) && F::regular(s)) {
+            const T y = F::rsqrt_pos(s);
+            c.Ka = A::mul(ph.K, A::mul(s, y));
+            c.iKa = A::mul(ph.iK, y);
+        } else {
+            c.Ka = A::mul(ph.K, A::sqrt(s));
+            c.iKa = A::rcp(c.Ka);
+        }
+        c.mu = A::mul(c.u, c.r);
+        c.mv = A::mul(c.v, c.r);
+        c.eup = F::fma(A::mul(A::half, c.r), temp, A::mul(c.p, ph.divgamma));
+        return c;
+    }
     const T inv = A::rcp(ur);
     c.r = ur;
     c.u = A::mul(uu, inv);
@@ -132,7 +239,7 @@ template <class T> __device__ __forceinline__ FaceIn<T> mirror(const FaceIn<T> &
 }
 
 // compute_fluxes, hydro2d/kernel.cxx:74-118, from cached per-cell quantities.
-template <class T>
+template <class T, bool kF = false>
 __device__ __forceinline__ Flux2<T> face_flux(const FaceIn<T> &L, const FaceIn<T> &R, const Phys<T> &ph)
 {
     using A = Ar<T>;
@@ -141,6 +248,18 @@ __device__ __forceinline__ Flux2<T> face_flux(const FaceIn<T> &L, const FaceIn<T
     const bool right = ph.kneg ? (R.Ka < L.Ka) : (L.Ka < R.Ka);
     const T a = right ? R.Ka : L.Ka;
     const T diva = right ? R.iKa : L.iKa;
+    if constexpr (kF) {
+        using F = Fu<T>;
+        const T us = A::mul(A::half, F::fma(-diva, A::sub(R.p, L.p), A::add(L.un, R.un)));
+        const T ps = A::mul(A::half, F::fma(-a, A::sub(R.un, L.un), A::add(L.p, R.p)));
+        const bool up = us >= T(0);
+        Flux2<T> F2;
+        F2.r = A::mul(up ? L.r : R.r, us);
+        F2.n = F::fma(up ? L.mn : R.mn, us, ps);
+        F2.t = A::mul(up ? L.mt : R.mt, us);
+        F2.E = F::fma(up ? L.eup : R.eup, us, A::mul(ps, us));
+        return F2;
+    }
     const T us = A::mul(A::half, A::sub(A::add(L.un, R.un), A::mul(diva, A::sub(R.p, L.p))));
     const T ps = A::mul(A::half, A::sub(A::add(L.p, R.p), A::mul(a, A::sub(R.un, L.un))));
     const bool up = us >= T(0);
@@ -163,12 +282,22 @@ template <class T> struct Upd2 {
     T r, u, v, E, speed;
 };
 
-template <class T>
+template <class T, bool kF = false>
 __device__ __forceinline__ Upd2<T> update2(T ur, T uu, T uv, T uE, const Flux2<T> &fx_lo, const Flux2<T> &fx_hi,
                                            const Flux2<T> &fy_lo, const Flux2<T> &fy_hi, T DtDx, T DtDy,
                                            const Phys<T> &ph)
 {
     using A = Ar<T>;
+    if constexpr (kF) {
+        using F = Fu<T>;
+        Upd2<T> o;
+        o.r = F::fma(DtDy, A::sub(fy_lo.r, fy_hi.r), F::fma(DtDx, A::sub(fx_lo.r, fx_hi.r), ur));
+        o.u = F::fma(DtDy, A::sub(fy_lo.t, fy_hi.t), F::fma(DtDx, A::sub(fx_lo.n, fx_hi.n), uu));
+        o.v = F::fma(DtDy, A::sub(fy_lo.n, fy_hi.n), F::fma(DtDx, A::sub(fx_lo.t, fx_hi.t), uv));
+        o.E = F::fma(DtDy, A::sub(fy_lo.E, fy_hi.E), F::fma(DtDx, A::sub(fx_lo.E, fx_hi.E), uE));
+        o.speed = T(0);
+        return o;
+    }
     const T x_r = A::mul(DtDx, A::sub(fx_lo.r, fx_hi.r));
     const T x_u = A::mul(DtDx, A::sub(fx_lo.n, fx_hi.n));
     const T x_v = A::mul(DtDx, A::sub(fx_lo.t, fx_hi.t));
@@ -187,9 +316,17 @@ __device__ __forceinline__ Upd2<T> update2(T ur, T uu, T uv, T uE, const Flux2<T
 }
 
 // Signal speed c_s + |u| of a 2D state, hydro2d/kernel.cxx:287-309.
-template <class T> __device__ __forceinline__ T speed2(T r, T ru, T rv, T E, const Phys<T> &ph)
+template <class T, bool kF = false> __device__ __forceinline__ T speed2(T r, T ru, T rv, T E, const Phys<T> &ph)
 {
     using A = Ar<T>;
+    if constexpr (kF) {
+        using F = Fu<T>;
+        const T inv = F::rcp(r);
+        const T qu = A::mul(ru, inv), qv = A::mul(rv, inv);
+        const T temp = F::fma(qv, qv, A::mul(qu, qu));
+        const T p = A::mul(A::mul(ph.gm1, r), F::fma(-A::half, temp, A::mul(E, inv)));
+        return A::add(F::sqrt(A::mul(A::mul(ph.gamma, p), inv)), F::sqrt(temp));
+    }
     const T inv = A::rcp(r);
     const T qu = A::mul(ru, inv);
     const T qv = A::mul(rv, inv);
@@ -237,11 +374,36 @@ template <class T> struct Cell3 {
     T r, u, v, w, p, Ka, iKa, mu, mv, mw, eup_xy, eup_z;
 };
 
-template <class T>
+template <class T, bool kF = false>
 __device__ __forceinline__ Cell3<T> make_cell3(T ur, T uu, T uv, T uw, T uE, const Phys<T> &ph)
 {
     using A = Ar<T>;
     Cell3<T> c;
+    if constexpr (kF) {
+        using F = Fu<T>;
+        const T inv = F::rcp(ur);
+        c.r = ur;
+        c.u = A::mul(uu, inv);
+        c.v = A::mul(uv, inv);
+        c.w = A::mul(uw, inv);
+        const T temp = F::fma(c.w, c.w, F::fma(c.v, c.v, A::mul(c.u, c.u)));
+        c.p = A::mul(A::mul(ph.gm1, ur), F::fma(-A::half, temp, A::mul(uE, inv)));
+        const T s = A::mul(A::mul(ph.gamma, c.p), c.r);
+        if (s > T(0) && F::regular(s)) {
+            const T y = F::rsqrt_pos(s);
+            c.Ka = A::mul(ph.K, A::mul(s, y));
+            c.iKa = A::mul(ph.iK, y);
+        } else {
+            c.Ka = A::mul(ph.K, A::sqrt(s));
+            c.iKa = A::rcp(c.Ka);
+        }
+        c.mu = A::mul(c.u, c.r);
+        c.mv = A::mul(c.v, c.r);
+        c.mw = A::mul(c.w, c.r);
+        c.eup_xy = F::fma(A::mul(A::half, c.r), temp, A::mul(c.p, ph.divgamma));
+        c.eup_z = c.eup_xy;
+        return c;
+    }
     const T inv = A::rcp(ur);
     c.r = ur;
     c.u = A::mul(uu, inv);
@@ -284,13 +446,26 @@ template <class T> __device__ __forceinline__ FaceIn3<T> mirror3(const FaceIn3<T
 }
 
 // compute_fluxes, hydro3d/kernel.cxx:79-130
-template <class T>
+template <class T, bool kF = false>
 __device__ __forceinline__ Flux3<T> face_flux3(const FaceIn3<T> &L, const FaceIn3<T> &R, const Phys<T> &ph)
 {
     using A = Ar<T>;
     const bool right = ph.kneg ? (R.Ka < L.Ka) : (L.Ka < R.Ka);
     const T a = right ? R.Ka : L.Ka;
     const T diva = right ? R.iKa : L.iKa;
+    if constexpr (kF) {
+        using F = Fu<T>;
+        const T us = A::mul(A::half, F::fma(-diva, A::sub(R.p, L.p), A::add(L.un, R.un)));
+        const T ps = A::mul(A::half, F::fma(-a, A::sub(R.un, L.un), A::add(L.p, R.p)));
+        const bool up = us >= T(0);
+        Flux3<T> F3;
+        F3.r = A::mul(up ? L.r : R.r, us);
+        F3.n = F::fma(up ? L.mn : R.mn, us, ps);
+        F3.t1 = A::mul(up ? L.mt1 : R.mt1, us);
+        F3.t2 = A::mul(up ? L.mt2 : R.mt2, us);
+        F3.E = F::fma(up ? L.eup : R.eup, us, A::mul(ps, us));
+        return F3;
+    }
     const T us = A::mul(A::half, A::sub(A::add(L.un, R.un), A::mul(diva, A::sub(R.p, L.p))));
     const T ps = A::mul(A::half, A::sub(A::add(L.p, R.p), A::mul(a, A::sub(R.un, L.un))));
     const bool up = us >= T(0);
@@ -314,13 +489,29 @@ template <class T> struct Upd3 {
 
 // hydro3d/kernel.cxx:330-394. Slot routing per direction: x (n=u, t1=v, t2=w),
 // y (n=v, t1=u, t2=w), z (n=w, t1=v, t2=u).
-template <class T>
+template <class T, bool kF = false>
 __device__ __forceinline__ Upd3<T> update3(T ur, T uu, T uv, T uw, T uE, const Flux3<T> &fx_lo,
                                            const Flux3<T> &fx_hi, const Flux3<T> &fy_lo, const Flux3<T> &fy_hi,
                                            const Flux3<T> &fz_lo, const Flux3<T> &fz_hi, T DtDx, T DtDy, T DtDz,
                                            const Phys<T> &ph)
 {
     using A = Ar<T>;
+    if constexpr (kF) {
+        using F = Fu<T>;
+        Upd3<T> o;
+        o.r = F::fma(DtDz, A::sub(fz_lo.r, fz_hi.r),
+                     F::fma(DtDy, A::sub(fy_lo.r, fy_hi.r), F::fma(DtDx, A::sub(fx_lo.r, fx_hi.r), ur)));
+        o.u = F::fma(DtDz, A::sub(fz_lo.t2, fz_hi.t2),
+                     F::fma(DtDy, A::sub(fy_lo.t1, fy_hi.t1), F::fma(DtDx, A::sub(fx_lo.n, fx_hi.n), uu)));
+        o.v = F::fma(DtDz, A::sub(fz_lo.t1, fz_hi.t1),
+                     F::fma(DtDy, A::sub(fy_lo.n, fy_hi.n), F::fma(DtDx, A::sub(fx_lo.t1, fx_hi.t1), uv)));
+        o.w = F::fma(DtDz, A::sub(fz_lo.n, fz_hi.n),
+                     F::fma(DtDy, A::sub(fy_lo.t2, fy_hi.t2), F::fma(DtDx, A::sub(fx_lo.t2, fx_hi.t2), uw)));
+        o.E = F::fma(DtDz, A::sub(fz_lo.E, fz_hi.E),
+                     F::fma(DtDy, A::sub(fy_lo.E, fy_hi.E), F::fma(DtDx, A::sub(fx_lo.E, fx_hi.E), uE)));
+        o.speed = T(0);
+        return o;
+    }
     const T x_r = A::mul(DtDx, A::sub(fx_lo.r, fx_hi.r));
     const T x_u = A::mul(DtDx, A::sub(fx_lo.n, fx_hi.n));
     const T x_v = A::mul(DtDx, A::sub(fx_lo.t1, fx_hi.t1));
@@ -347,9 +538,18 @@ __device__ __forceinline__ Upd3<T> update3(T ur, T uu, T uv, T uw, T uE, const F
 }
 
 // Signal speed c_s + |u| of a 3D state, hydro3d/kernel.cxx:367-390.
-template <class T> __device__ __forceinline__ T speed3(T r, T ru, T rv, T rw, T E, const Phys<T> &ph)
+template <class T, bool kF = false>
+__device__ __forceinline__ T speed3(T r, T ru, T rv, T rw, T E, const Phys<T> &ph)
 {
     using A = Ar<T>;
+    if constexpr (kF) {
+        using F = Fu<T>;
+        const T inv = F::rcp(r);
+        const T qu = A::mul(ru, inv), qv = A::mul(rv, inv), qw = A::mul(rw, inv);
+        const T temp = F::fma(qw, qw, F::fma(qv, qv, A::mul(qu, qu)));
+        const T p = A::mul(A::mul(ph.gm1, r), F::fma(-A::half, temp, A::mul(E, inv)));
+        return A::add(F::sqrt(A::mul(A::mul(ph.gamma, p), inv)), F::sqrt(temp));
+    }
     const T inv = A::rcp(r);
     const T qu = A::mul(ru, inv), qv = A::mul(rv, inv), qw = A::mul(rw, inv);
     const T temp = A::add(A::add(A::mul(qu, qu), A::mul(qv, qv)), A::mul(qw, qw));

@@ -70,7 +70,7 @@ struct March2 {
 // (16-byte row pitch). kTma = false: each lane copies its own cell with cp.async (any
 // pitch; 8-byte (FP32) or 16-byte (FP64) aligned arrays), so a lane reads only what it
 // copied and the ring needs no barrier.
-template <bool kEdge, bool kTma, class T, class Sink>
+template <bool kEdge, bool kTma, bool kF, class T, class Sink>
 __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tmr, const CUtensorMap *tmu,
                                               const March2 &g, T *rhoE_n, T *uv_n, const Phys<T> &ph, T DtDx,
                                               T DtDy, unsigned &ld, Sink &sink)
@@ -137,7 +137,7 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
             a = mk2<T>(T(1), T(1));
             b = mk2<T>(T(0), T(0));
         }
-        const Cell2<T> P = make_cell2<T>(a.x, b.x, b.y, a.y, ph);
+        const Cell2<T> P = make_cell2<T, kF>(a.x, b.x, b.y, a.y, ph);
         const bool yrow = (m >= 1) && (m <= nrows - 2);
         if (yrow) {
             const FaceIn<T> me = face_y(P);
@@ -154,12 +154,12 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
 
         if (m >= 1) {
             // x face (row n-1 | row n) of this column; then the update of row n-1
-            const Flux2<T> fxhi = face_flux(face_x(Pm), face_x(P), ph);
+            const Flux2<T> fxhi = face_flux<T, kF>(face_x(Pm), face_x(P), ph);
             if (m >= 2 && interior) {
                 // row n-1's left face is lane t-1's right face of that row
                 const V2 f0 = S.xF[(m - 1) & 1][0][t], f1 = S.xF[(m - 1) & 1][1][t];
                 const Flux2<T> fyl{f0.x, f0.y, f1.x, f1.y};
-                const Upd2<T> o = update2(Ur, Uu, Uv, UE, fxlo, fxhi, fyl, fyr, DtDx, DtDy, ph);
+                const Upd2<T> o = update2<T, kF>(Ur, Uu, Uv, UE, fxlo, fxhi, fyl, fyr, DtDx, DtDy, ph);
                 const long long c = (long long)(g.i0 + m - 2) * g.ys + j;
                 reinterpret_cast<V2 *>(rhoE_n)[c] = mk2<T>(o.r, o.E);
                 reinterpret_cast<V2 *>(uv_n)[c] = mk2<T>(o.u, o.v);
@@ -178,7 +178,7 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
                 if (j == 0) L = mirror(R);       // wall at j = 1/2
                 if (j == g.nb_y) R = mirror(me); // wall at j = NB_Y + 1/2
             }
-            fyr = face_flux(L, R, ph);
+            fyr = face_flux<T, kF>(L, R, ph);
             S.xF[m & 1][0][t + 1] = mk2<T>(fyr.r, fyr.n);
             S.xF[m & 1][1][t + 1] = mk2<T>(fyr.t, fyr.E);
         }
@@ -200,15 +200,15 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
 }
 
 // One strip march: the lean form away from the Y walls, the general one at them (the
-// choice is uniform over the block).
-template <class T, bool kTma = true, class Sink>
+// choice is uniform over the block). kF: fused arithmetic (hydro_math.cuh).
+template <class T, bool kTma = true, bool kF = false, class Sink>
 __device__ __forceinline__ bool march2d(Smem2<T> &S, const CUtensorMap *tmr, const CUtensorMap *tmu, const March2 &g,
                                         T *rhoE_n, T *uv_n, const Phys<T> &ph, T DtDx, T DtDy, unsigned &ld,
                                         Sink &&sink)
 {
     if (g.jbase >= 1 && g.jbase + kStripNT - 1 <= g.nb_y)
-        return march2d_strip<false, kTma>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
-    return march2d_strip<true, kTma>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
+        return march2d_strip<false, kTma, kF>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
+    return march2d_strip<true, kTma, kF>(S, tmr, tmu, g, rhoE_n, uv_n, ph, DtDx, DtDy, ld, sink);
 }
 
 } // namespace hydro

@@ -4,9 +4,14 @@
 //
 // One block of 8 (FP64) or 16 (FP32) warps covers a (warps) y x 32 z tile of columns
 // starting at (jbase, kbase): the interior columns plus a one-cell halo ring. Each X plane
-// of the tile is copied into a k3Stages-deep shared-memory ring with cp.async (any
-// alignment of the interleaved pairs/triples): in FP64 by every lane for its own cell, in
-// FP32 by the two halo-row warps for the whole tile. Each lane converts its cell to
+// of the tile arrives in a k3Stages-deep shared-memory ring, in one of two forms:
+//  - tensor maps (kTma): one thread issues two 3D TMA tile loads per plane (the (rho, E)
+//    pairs and the momentum triples of the tile's rows, x = the interleaved components of
+//    32 cells, y = 8 rows, z = the plane) completing on the stage's mbarrier; needs a row
+//    pitch of a multiple of 16 bytes (FP64 with even NB_Z) and even kbase;
+//  - per-lane copies: cp.async of any alignment of the interleaved pairs/triples, in FP64
+//    by every lane for its own cell, in FP32 by the two halo-row warps for the whole tile.
+// Each lane converts its cell to
 // primitives once and publishes them as 16-byte pairs (double-buffered by plane parity;
 // one barrier per plane). Per plane a lane computes one x face (registers), one z face (the next lane's
 // cell from shared memory, the flux back by shuffles) and one y face (the warp above's
@@ -41,7 +46,15 @@ template <class T> __device__ __forceinline__ typename Vec2<T>::type pair3(T a, 
 
 template <class T> struct Smem3 {
     using V2 = typename Vec2<T>::type;
-    T st[k3Stages][5][k3NT<T>]; // per plane: rho, E, rho_u, rho_v, rho_w
+    union {
+        T st[k3Stages][5][k3NT<T>]; // per-lane copies, per plane: rho, E, rho_u, rho_v, rho_w
+        struct {                    // tensor-map boxes in tile order (lane t = 32 row + column)
+            T r[k3Stages][k3NT<T>][2]; // (rho, E)
+            T u[k3Stages][k3NT<T>][3]; // (rho u, rho v, rho w)
+        } tm;
+    };
+    uint64_t full[k3Stages]; // tensor-map form: stage s holds its plane
+    int abort;
     // each lane's cell by plane parity, as pairs (r,p) (Ka,iKa) (v,w) (mu,mv) (mw,eup_xy)
     // (eup_z,-): the warp below reads its y-face inputs, the previous lane its z-face inputs
     V2 xP[2][6][k3NT<T>];
@@ -72,9 +85,28 @@ struct March3 {
 // kEdge = false: a tile whose every lane holds a real cell (1 <= j <= NB_Y,
 // 1 <= k <= NB_Z) and whose faces used by interior lanes touch no wall; it needs neither
 // the unit-state substitution nor the wall mirrors. kEdge = true: any tile.
-template <bool kEdge, class T, class Sink>
-__device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
-                                             const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &sink)
+// Tensor maps of the two input arrays for the kTma form (null otherwise).
+struct Tmaps3 {
+    const CUtensorMap *r = nullptr, *u = nullptr;
+};
+
+// One-time set-up of the stage barriers of the tensor-map form (thread 0), then a block
+// barrier.
+template <class T> __device__ __forceinline__ void march3d_init(Smem3<T> &S)
+{
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < k3Stages; ++s) mbar_init(&S.full[s], 1);
+        fence_mbar_init();
+        S.abort = 0;
+    }
+    __syncthreads();
+}
+
+// Returns false when a bounded barrier wait of the tensor-map form gave up.
+template <bool kEdge, bool kF, bool kTma, class T, class Sink>
+__device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
+                                             const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz,
+                                             const Tmaps3 &tm, Sink &sink)
 {
     constexpr unsigned FULL = 0xffffffffu;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -100,6 +132,16 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
     const bool kin = !kEdge || (k <= g.nb_z + 1);
 
     __syncthreads(); // the previous march of this block is done with the stages and exchange buffers
+    constexpr uint32_t kPlaneBytes = (uint32_t)(5 * k3NT<T> * sizeof(T));
+    // tensor-map form: thread 0 loads plane m into stage m % k3Stages (a single march per
+    // block: stage s completes its phase (m / k3Stages) & 1)
+    auto issue_tma = [&](int m) {
+        const int s = m % k3Stages;
+        const int plane = g.xwrap ? wrap_plane(g.i0 - 1 + m, g.nb_x) : g.i0 - 1 + m;
+        mbar_arrive_expect_tx(&S.full[s], kPlaneBytes);
+        tma_load_3d(&S.tm.r[s][0][0], tm.r, 2 * g.kbase, g.jbase, plane, &S.full[s]);
+        tma_load_3d(&S.tm.u[s][0][0], tm.u, 3 * g.kbase, g.jbase, plane, &S.full[s]);
+    };
     auto issue = [&](int m) { // loading lanes only
         const int s = m % k3Stages;
         if (m < nplanes) {
@@ -122,38 +164,61 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
         }
         cp_async_commit();
     };
-    if (loader) {
+    if constexpr (kTma) {
+        if (t == 0)
+            for (int m = 0; m < k3Stages - 1 && m < nplanes; ++m) issue_tma(m);
+    } else {
+        if (loader) {
 #pragma unroll
-        for (int m = 0; m < k3Stages - 1; ++m) issue(m);
-    }
-    if (kHaloLoads) {
-        if (loader) cp_async_wait<k3Stages - 2>(); // plane 0 landed
-        __syncthreads();                          // plane 0 visible to every lane
+            for (int m = 0; m < k3Stages - 1; ++m) issue(m);
+        }
+        if (kHaloLoads) {
+            if (loader) cp_async_wait<k3Stages - 2>(); // plane 0 landed
+            __syncthreads();                          // plane 0 visible to every lane
+        }
     }
 
     Cell3<T> Pm{};
     T Ur = 0, Uu = 0, Uv = 0, Uw = 0, UE = 0;
     Flux3<T> fxlo{};
+    int m = 0;
 #pragma unroll 2
-    for (int m = 0; m < nplanes; ++m) {
-        // the stage of plane m-1 is refilled with plane m+k3Stages-1. Halo loads: plane m
-        // landed before the previous plane's barrier, and plane m+1 must land before this
-        // plane's. Own loads: each lane waits for its own copy of plane m.
-        if (loader) issue(m + k3Stages - 1);
-        if (kHaloLoads) {
-            if (loader) cp_async_wait<k3Stages - 2>();
-        } else {
-            cp_async_wait<k3Stages - 1>();
-        }
+    for (; m < nplanes; ++m) {
+        // the stage of plane m-1 is refilled with plane m+k3Stages-1 (every lane read it
+        // before the previous plane's barrier). Tensor maps: every lane waits for the
+        // stage's barrier. Halo loads: plane m landed before the previous plane's barrier,
+        // and plane m+1 must land before this plane's. Own loads: each lane waits for its
+        // own copy of plane m.
         const int s = m % k3Stages;
-        T ur = S.st[s][0][t], uE = S.st[s][1][t];
-        T uu = S.st[s][2][t], uv = S.st[s][3][t], uw = S.st[s][4][t];
+        T ur, uE, uu, uv, uw;
+        if constexpr (kTma) {
+            if (t == 0 && m + k3Stages - 1 < nplanes) issue_tma(m + k3Stages - 1);
+            if (!mbar_wait_bounded(&S.full[s], (uint32_t)(m / k3Stages) & 1u)) S.abort = 1;
+            const typename Smem3<T>::V2 a = *reinterpret_cast<const typename Smem3<T>::V2 *>(&S.tm.r[s][t][0]);
+            ur = a.x;
+            uE = a.y;
+            uu = S.tm.u[s][t][0];
+            uv = S.tm.u[s][t][1];
+            uw = S.tm.u[s][t][2];
+        } else {
+            if (loader) issue(m + k3Stages - 1);
+            if (kHaloLoads) {
+                if (loader) cp_async_wait<k3Stages - 2>();
+            } else {
+                cp_async_wait<k3Stages - 1>();
+            }
+            ur = S.st[s][0][t];
+            uE = S.st[s][1][t];
+            uu = S.st[s][2][t];
+            uv = S.st[s][3][t];
+            uw = S.st[s][4][t];
+        }
         if (kEdge && !real) {
             ur = T(1);
             uE = T(1);
             uu = uv = uw = T(0);
         }
-        const Cell3<T> P = make_cell3<T>(ur, uu, uv, uw, uE, ph);
+        const Cell3<T> P = make_cell3<T, kF>(ur, uu, uv, uw, uE, ph);
         {
             typename Smem3<T>::V2 *x = &S.xP[m & 1][0][t];
             x[0 * k3NT<T>] = pair3<T>(P.r, P.p);
@@ -172,7 +237,7 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
                 if (j == 0) L = mirror3(nb);
                 if (j == g.nb_y) R = mirror3(me);
             }
-            return face_flux3(L, R, ph);
+            return face_flux3<T, kF>(L, R, ph);
         };
         // +z face of (k | k+1): the next lane's cell from the exchange buffer (lane 31
         // reads the next warp's lane 0, a face no interior lane uses)
@@ -184,7 +249,7 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
                 if (k == 0) L = mirror3(nz);
                 if (k == g.nb_z) R = mirror3(mz);
             }
-            return face_flux3(L, R, ph);
+            return face_flux3<T, kF>(L, R, ph);
         };
         auto publish_y = [&](const Flux3<T> &fy) {
             S.xF[m & 1][0][t] = pair3<T>(fy.r, fy.n);
@@ -198,7 +263,7 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
             // can interleave); the halo row above them only its +y face
             Flux3<T> fy{}, fz{};
             if (iwarp) {
-                fxhi = face_flux3(face3_x(Pm), face3_x(P), ph);
+                fxhi = face_flux3<T, kF>(face3_x(Pm), face3_x(P), ph);
                 fy = yface();
                 fz = zface();
                 publish_y(fy);
@@ -207,6 +272,7 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
                 publish_y(fy);
             }
             __syncthreads(); // +y faces of this plane published
+            if (kTma && S.abort) break;
             if (iwarp) {
                 Flux3<T> fzl;
                 fzl.r = __shfl_up_sync(FULL, fz.r, 1);
@@ -218,7 +284,7 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
                     const auto a0 = S.xF[m & 1][0][t - 32], a1 = S.xF[m & 1][1][t - 32];
                     const Flux3<T> fyl{a0.x, a0.y, a1.x, a1.y, S.xFE[m & 1][t - 32]};
                     const Upd3<T> o =
-                        update3(Ur, Uu, Uv, Uw, UE, fxlo, fxhi, fyl, fy, fzl, fz, DtDx, DtDy, DtDz, ph);
+                        update3<T, kF>(Ur, Uu, Uv, Uw, UE, fxlo, fxhi, fyl, fy, fzl, fz, DtDx, DtDy, DtDz, ph);
                     const long long c = (long long)(g.i0 + m - 2) * g.zy + colofs;
                     rhoE_n[2 * c] = o.r;
                     rhoE_n[2 * c + 1] = o.E;
@@ -229,28 +295,43 @@ __device__ __forceinline__ void march3d_tile(Smem3<T> &S, const T *rhoE, const T
                 }
             }
         } else {
-            if (m >= 1 && iwarp) fxhi = face_flux3(face3_x(Pm), face3_x(P), ph);
+            if (m >= 1 && iwarp) fxhi = face_flux3<T, kF>(face3_x(Pm), face3_x(P), ph);
             __syncthreads(); // keep one barrier per plane: publishes this plane's xP
+            if (kTma && S.abort) break;
         }
         fxlo = fxhi;
         Pm = P;
         Ur = ur; Uu = uu; Uv = uv; Uw = uw; UE = uE;
     }
-    cp_async_wait<0>();
+    if constexpr (kTma) {
+        if (m < nplanes) {
+            // gave up on a barrier: wait (bounded) for the loads still in flight before the
+            // block's shared memory is released
+            if (t == 0)
+                for (int q = m; q < nplanes && q < m + k3Stages; ++q)
+                    (void)mbar_wait_bounded(&S.full[q % k3Stages], (uint32_t)(q / k3Stages) & 1u);
+            __syncthreads();
+            return false;
+        }
+    } else {
+        cp_async_wait<0>();
+    }
+    return true;
 }
 
 // One tile march: the lean form for tiles away from walls and ghosts, the general one
-// elsewhere (the choice is uniform over the block).
-template <class T, class Sink>
-__device__ __forceinline__ void march3d(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
-                                        const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &&sink)
+// elsewhere (the choice is uniform over the block). kF: fused arithmetic (hydro_math.cuh).
+// kTma: planes staged by the tensor maps `tm` (march3d_init first); else per-lane copies.
+// Returns false when a bounded barrier wait gave up.
+template <class T, bool kF = false, bool kTma = false, class Sink>
+__device__ __forceinline__ bool march3d(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
+                                        const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &&sink,
+                                        const Tmaps3 &tm = Tmaps3{})
 {
     const bool inner =
         g.jbase >= 1 && g.jbase + k3Warps<T> - 1 <= g.nb_y && g.kbase >= 1 && g.kbase + 31 <= g.nb_z;
-    if (inner)
-        march3d_tile<false>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
-    else
-        march3d_tile<true>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
+    if (inner) return march3d_tile<false, kF, kTma>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, tm, sink);
+    return march3d_tile<true, kF, kTma>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, tm, sink);
 }
 
 } // namespace hydro
