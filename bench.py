@@ -158,11 +158,11 @@ def energy_entry(joules, seconds, cell_updates):
 
 
 # -------------------------------------------------------------- GPU measurements ---
-def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0, meter=None):
+def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0, meter=None, arith=None):
     """Host loop with the state resident on the device; CUDA events on the launching
     stream: total time of `steps` steps and per-step kernel time (and the energy of the
     timed steps when a meter is given)."""
-    run = hb.BlastRun(nb, T, kernel=kernel)
+    run = hb.BlastRun(nb, T, kernel=kernel, arith=arith)
     for _ in range(warmup):
         run.step()
     torch.cuda.synchronize()
@@ -462,46 +462,72 @@ def bench_serving(hb, torch, rates=(10.0, 100.0, 1000.0), nreq=8, seed=0, max_wa
 
 
 # ------------------------------------------------------------ FP32 vs FP64 accuracy ---
-def fp32_accuracy(hb, torch, nb, steps=100):
-    """The plain path in FP32 and in FP64 from the same blast for `steps` iterations;
-    relative L1 (sum |a - b| / sum |b|) and L-infinity (max |a - b| / max |b|) of rho, p
-    and the velocities of the FP32 result against the FP64 one, which is bit-identical
-    to the reference's FP64 kernel (the GPU parity tests)."""
+def accuracy_vs_strict_fp64(hb, torch, nb, steps=100, variants=(("fp32_strict", np.float32, "strict"),
+                                                                  ("fp32_fused", np.float32, "fused"),
+                                                                  ("fp64_fused", np.float64, "fused"))):
+    """The plain path from the same blast for `steps` iterations in strict FP64 (bit-identical
+    to the reference's FP64 kernel: the GPU parity tests) and in each variant; per variant
+    and field (rho, p and the velocities) the relative L1 (sum |a - b| / sum |b|), the
+    relative L-infinity (max |a - b| / max |b|) and the max pointwise relative error with
+    the denominator floored at 1e-12 max |b| (max |a - b| / max(|b|, 1e-12 max |b|))."""
+    ref = hb.BlastRun(nb, np.float64, arith="strict").run(float("inf"), steps)
+    out = dict(steps=steps, grid="x".join(map(str, nb)),
+               reference="strict FP64 plain path (bit-identical to the oracle)")
+    for name, T, arith in variants:
+        r = hb.BlastRun(nb, T, arith=arith).run(float("inf"), steps)
+        out[name] = _field_errors(torch, nb, r, ref)
+        out[name]["same_iterations"] = r.it == ref.it
+        del r
+        torch.cuda.empty_cache()
+    del ref
+    torch.cuda.empty_cache()
+    return out
+
+
+def _field_errors(torch, nb, run, ref):
+    """Errors of run's final state against ref's, field by field, on the device in chunks."""
     dim = len(nb)
-    runs = {}
-    for T in (np.float64, np.float32):
-        r = hb.BlastRun(nb, T).run(float("inf"), steps)
-        runs[T] = r
+    runs = {"a": run, "b": ref}
     gm1 = 0.4
-    out = dict(steps=steps, grid="x".join(map(str, nb)), reference="plain FP64 path (bit-identical to the oracle)")
+    out = {}
     names = ["rho", "p", "u", "v", "w"][:dim + 2]
-    acc = {n: [0.0, 0.0, 0.0, 0.0] for n in names}  # sum|d|, sum|b|, max|d|, max|b|
+    # sum|d|, sum|b|, max|d|, max|b|, and per chunk the floored ratio needs max|b| first:
+    # two passes (the first for max|b|)
+    acc = {n: [0.0, 0.0, 0.0, 0.0, 0.0] for n in names}
     nplane = int(np.prod([n + 2 for n in nb[1:]]))
     inner = tuple(slice(1, n + 1) for n in nb[1:])
     nv = dim
-    rows = max(1, int(2e8 // nplane))
-    for i0 in range(1, nb[0] + 1, rows):
-        i1 = min(nb[0] + 1, i0 + rows)
-        fields = {}
-        for T, r in runs.items():
-            rhoE = r.cur[0][2 * nplane * i0:2 * nplane * i1].double().view(i1 - i0, *[n + 2 for n in nb[1:]], 2)
-            mom = r.cur[1][nv * nplane * i0:nv * nplane * i1].double().view(i1 - i0, *[n + 2 for n in nb[1:]], nv)
-            rho = rhoE[(slice(None),) + inner + (0,)]
-            E = rhoE[(slice(None),) + inner + (1,)]
-            m = mom[(slice(None),) + inner]
-            vel = m / rho.unsqueeze(-1)
-            p = gm1 * (E - 0.5 * (m * vel).sum(-1))
-            fields[T] = [rho, p] + [vel[..., c] for c in range(nv)]
-        for n, a, b in zip(names, fields[np.float32], fields[np.float64]):
+    rows = max(1, int(1e8 // nplane))
+
+    def chunks():
+        for i0 in range(1, nb[0] + 1, rows):
+            i1 = min(nb[0] + 1, i0 + rows)
+            fields = {}
+            for key, r in runs.items():
+                rhoE = r.cur[0][2 * nplane * i0:2 * nplane * i1].double().view(i1 - i0, *[n + 2 for n in nb[1:]], 2)
+                mom = r.cur[1][nv * nplane * i0:nv * nplane * i1].double().view(i1 - i0, *[n + 2 for n in nb[1:]],
+                                                                               nv)
+                rho = rhoE[(slice(None),) + inner + (0,)]
+                E = rhoE[(slice(None),) + inner + (1,)]
+                m = mom[(slice(None),) + inner]
+                vel = m / rho.unsqueeze(-1)
+                p = gm1 * (E - 0.5 * (m * vel).sum(-1))
+                fields[key] = [rho, p] + [vel[..., c] for c in range(nv)]
+            yield fields
+
+    for fields in chunks():
+        for n, a, b in zip(names, fields["a"], fields["b"]):
             d = (a - b).abs()
             acc[n][0] += float(d.sum())
             acc[n][1] += float(b.abs().sum())
             acc[n][2] = max(acc[n][2], float(d.max()))
             acc[n][3] = max(acc[n][3], float(b.abs().max()))
-    for n, (sd, sb, md, mb) in acc.items():
-        out[n] = dict(rel_l1=sd / sb if sb > 0 else 0.0, rel_linf=md / mb if mb > 0 else 0.0)
-    del runs
-    torch.cuda.empty_cache()
+    for fields in chunks():
+        for n, a, b in zip(names, fields["a"], fields["b"]):
+            den = b.abs().clamp(min=1e-12 * acc[n][3]) if acc[n][3] > 0 else b.abs() + 1.0
+            acc[n][4] = max(acc[n][4], float(((a - b).abs() / den).max()))
+    for n, (sd, sb, md, mb, mr) in acc.items():
+        out[n] = dict(rel_l1=sd / sb if sb > 0 else 0.0, rel_linf=md / mb if mb > 0 else 0.0, max_rel_floored=mr)
     return out
 
 
@@ -640,6 +666,8 @@ def main():
     ap.add_argument("--batched-instances", type=int, default=256)
     ap.add_argument("--batched-steps", type=int, default=200)
     ap.add_argument("--batched-chunk", type=int, default=0, help="rows per work item (0: autotuned)")
+    ap.add_argument("--arith", default="strict", choices=["strict", "fused"],
+                    help="arithmetic of the headline plain-path case (the variants time both)")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="iterations of the FP32-vs-FP64 accuracy runs on the large grids")
@@ -721,7 +749,7 @@ def main():
     meter = EnergyMeter(uuid)
     sampler = ClockSampler(uuid)
     sampler.start()
-    r = bench_resident(hb, torch, nb, Tcase, args.steps, args.warmup, meter=meter)
+    r = bench_resident(hb, torch, nb, Tcase, args.steps, args.warmup, meter=meter, arith=args.arith)
     clocks = sampler.stop()
     barrier()
     total_ms = max_over_ranks(r["total_ms"])
@@ -749,12 +777,19 @@ def main():
 
     variants = {}
     if not args.no_variants and args.case == "2d_f64":
-        for name, vnb, T in (("2d_f32_40000x20000", nb, np.float32), ("3d_f64_512^3", (512, 512, 512), np.float64),
-                             ("3d_f32_512^3", (512, 512, 512), np.float32)):
+        n3 = (512, 512, 512)
+        other = "fused" if args.arith == "strict" else "strict"
+        for name, vnb, T, ar in ((f"2d_f64_40000x20000_{other}", nb, np.float64, other),
+                                 ("2d_f32_40000x20000_strict", nb, np.float32, "strict"),
+                                 ("2d_f32_40000x20000_fused", nb, np.float32, "fused"),
+                                 ("3d_f64_512^3_strict", n3, np.float64, "strict"),
+                                 ("3d_f64_512^3_fused", n3, np.float64, "fused"),
+                                 ("3d_f32_512^3_strict", n3, np.float32, "strict"),
+                                 ("3d_f32_512^3_fused", n3, np.float32, "fused")):
             barrier()
             vsampler = ClockSampler(uuid)
             vsampler.start()
-            vr = bench_resident(hb, torch, vnb, T, max(5, args.steps // 3), 3)
+            vr = bench_resident(hb, torch, vnb, T, max(5, args.steps // 3), 3, arith=ar)
             vclocks = vsampler.stop()
             barrier()
             vms = max_over_ranks(vr["total_ms"])
@@ -768,9 +803,9 @@ def main():
 
     accuracy = {}
     if rank == 0 and world == 1 and not args.no_accuracy and args.case == "2d_f64":
-        # the FP32 plain path against FP64 on the large grids, 100 iterations each
+        # FP32 and fused FP64 against strict FP64 on the large grids, 100 iterations each
         for name, vnb in (("2d_40000x20000", nb), ("3d_512^3", (512, 512, 512))):
-            accuracy[name] = fp32_accuracy(hb, torch, vnb, steps=args.accuracy_steps)
+            accuracy[name] = accuracy_vs_strict_fp64(hb, torch, vnb, steps=args.accuracy_steps)
 
     log = lambda msg: print(msg, file=sys.stderr, flush=True)
     batched = serving = None
@@ -815,8 +850,7 @@ def main():
             line["variants_gcell_s"] = {k: v["value"] for k, v in variants.items()}
             line["variants_frac"] = {k: v["frac"] for k, v in variants.items()}
         if accuracy:
-            line["fp32_vs_fp64"] = {k: {n: v[n] for n in ("rho", "p", "u", "v", "w") if n in v}
-                                    for k, v in accuracy.items()}
+            line["accuracy_vs_strict_fp64"] = accuracy
         line["energy"] = energy_entry(r["energy_j"], total_ms / 1e3, cells * args.steps)
         line["variants"] = variants
         line["batched"] = batched

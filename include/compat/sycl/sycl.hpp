@@ -101,6 +101,11 @@ class queue {
         // (a multi-rank --sdx run) instead of wrapping periodically in-kernel (one rank)
         const char *xg = std::getenv("HYDRO_B200_X_GHOSTS");
         q_.flags = (xg && std::strcmp(xg, "memory") == 0) ? HYDRO_X_GHOSTS_FROM_MEMORY : 0;
+        // HYDRO_B200_ARITH=fused / strict: the arithmetic of every step (the library's
+        // default when unset)
+        const char *ar = std::getenv("HYDRO_B200_ARITH");
+        if (ar && std::strcmp(ar, "fused") == 0) q_.flags |= HYDRO_ARITH_FUSED;
+        if (ar && std::strcmp(ar, "strict") == 0) q_.flags |= HYDRO_ARITH_STRICT;
     }
     template <class S> explicit queue(const S &) : queue() {}
 
