@@ -165,6 +165,7 @@ def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0, meter=None, arith=
     run = hb.BlastRun(nb, T, kernel=kernel, arith=arith)
     for _ in range(warmup):
         run.step()
+    shape = hb.last_launch_shape()
     torch.cuda.synchronize()
     j0 = meter.read() if meter else None
     stream = torch.cuda.current_stream()
@@ -186,6 +187,7 @@ def bench_resident(hb, torch, nb, T, steps, warmup, kernel=0, meter=None, arith=
     # an asynchronous step launches the update kernel and the signal-speed check kernel
     # (which returns at once unless the fused maximum fell under its skip threshold)
     res = dict(total_ms=total_ms, kernel_ms=kern_ms, kernel=int(info.kernel), it=run.it, launches_per_step=2,
+               shape=shape,
                energy_j=(j1 - j0) if (j0 is not None and j1 is not None) else None)
     del run
     torch.cuda.empty_cache()
@@ -544,6 +546,63 @@ def config_for(nb, T):
                 parallelism="replicas: one per GPU, no data-path collective")
 
 
+def bench_serving_sweep(hb, torch, rates=(10.0, 30.0, 100.0, 300.0, 1000.0), nreq=200, seed=0, plain=True,
+                        bound_requests=2000, bound_wall=240.0, max_wall=None, trace_path=None, log=print):
+    """The serving workload as configured: at each rate a seeded Poisson stream of `nreq`
+    mixed requests (each in its own precision) through the continuous-batching server
+    (150 GB budget) and, when `plain`, through the plain path one request at a time; then
+    one stream of `bound_requests` at the highest rate, whose states together exceed the
+    150 GB budget, through the server alone for at most `bound_wall` seconds (requests queue
+    for memory; latency covers the requests completed by then). The trace of every
+    stream (arrival, grid, blast parameters, t_end, precision) goes to `trace_path`."""
+    from hydro_b200.autotune import best_chunk
+    from hydro_b200.serving import Server, serve_plain, summarize
+    from hydro_b200.workloads import request_stream
+
+    def served(reqs, budget=150e9, wall_cap=max_wall):
+        srv = Server(hbm_budget=budget, steps_per_tick=8, chunk2d=best_chunk(2, np.float32),
+                     chunk3d=best_chunk(3, np.float32))
+        recs, wall = srv.serve(reqs, max_wall=wall_cap)
+        stats = dict(srv.stats)
+        srv.close()
+        torch.cuda.empty_cache()
+        out = summarize(recs, wall)
+        out["budget"] = stats
+        return out
+
+    def trace(reqs):
+        return [dict(rid=r.rid, arrival=r.arrival, nb=list(r.blast.nb), centre=list(r.blast.centre),
+                     radius=r.blast.radius, p_in=r.blast.p_in, p_out=r.blast.p_out, t_end=r.blast.t_end,
+                     dtype=np.dtype(r.dtype).name) for r in reqs]
+
+    res, traces = {}, {}
+    for rate in rates:
+        reqs = request_stream(rate, seed=seed, count=nreq)
+        traces[f"rate_{rate:g}"] = trace(reqs)
+        entry = dict(batched=served(reqs))
+        if plain:
+            recs, wall = serve_plain(reqs, max_wall=max_wall)
+            torch.cuda.empty_cache()
+            entry["plain_one_at_a_time"] = summarize(recs, wall)
+            entry["batched_over_plain"] = entry["batched"]["gcell_s"] / max(
+                entry["plain_one_at_a_time"]["gcell_s"], 1e-30)
+        res[f"rate_{rate:g}"] = entry
+        log(f"serving sweep rate {rate:g}/s: {json.dumps(entry)}")
+    if bound_requests:
+        rate = max(rates)
+        reqs = request_stream(rate, seed=seed + 1, count=bound_requests)
+        traces[f"budget_bound_rate_{rate:g}"] = trace(reqs)
+        # double-buffered states with ghosts (rows the engines pad to 16 bytes not counted)
+        need = sum(2 * int(np.prod([n + 2 for n in r.blast.nb])) * (2 + len(r.blast.nb)) * np.dtype(r.dtype).itemsize
+                   for r in reqs)
+        entry = dict(batched=served(reqs, wall_cap=bound_wall), total_state_bytes=need)
+        res[f"budget_bound_rate_{rate:g}"] = entry
+        log(f"serving budget-bound run: {json.dumps(entry)}")
+    if trace_path:
+        Path(trace_path).write_text(json.dumps(dict(seed=seed, streams=traces)))
+    return res
+
+
 # ------------------------------------------------------------------- kernel tour ---
 def bench_tour(hb, torch, hbm, reps=5, log=print):
     """Every kernel of the library on a case whose state is larger than L2 (126 MB), timed
@@ -668,6 +727,7 @@ def main():
     ap.add_argument("--batched-chunk", type=int, default=0, help="rows per work item (0: autotuned)")
     ap.add_argument("--arith", default="strict", choices=["strict", "fused"],
                     help="arithmetic of the headline plain-path case (the variants time both)")
+    ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes (no plain-path autotuning)")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="iterations of the FP32-vs-FP64 accuracy runs on the large grids")
@@ -676,6 +736,10 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=8)
     ap.add_argument("--serving-wall", type=float, default=20.0, help="cap per serving run, seconds")
     ap.add_argument("--no-serving-plain", action="store_true")
+    ap.add_argument("--serving-sweep", action="store_true",
+                    help="the serving workload as configured (rates 10..1000/s, 200 requests each, plus a "
+                         "budget-bound stream) instead of the plain-path benchmark; one JSON line")
+    ap.add_argument("--serving-trace", default=None, help="file for the sweep's request traces")
     ap.add_argument("--tour", action="store_true",
                     help="time every kernel of the library on a small case (one JSON line each) and exit")
     args = ap.parse_args()
@@ -733,6 +797,15 @@ def main():
     max_over_ranks, barrier = reps.max_over_ranks, reps.barrier
 
     hbm, peak_kind = peaks()
+    if args.serving_sweep:
+        if rank == 0:
+            sw = bench_serving_sweep(hb, torch, rates=tuple(args.serving_rates), nreq=args.serving_requests,
+                                     plain=not args.no_serving_plain, trace_path=args.serving_trace,
+                                     log=lambda m: print(m, file=sys.stderr, flush=True))
+            print(json.dumps(dict(serving_sweep=sw)), flush=True)
+        reps.barrier()
+        reps.close()
+        return
     if args.tour:
         if rank == 0:
             bench_tour(hb, torch, hbm, log=lambda m: print(m, flush=True))
@@ -744,6 +817,23 @@ def main():
     bpc = BYTES_PER_CELL[(dim, isz)]
     kname = f"strip{dim}d<{'double' if isz == 8 else 'float'}>"
 
+    tuned = {}
+    log = lambda msg: print(msg, file=sys.stderr, flush=True)
+
+    def tune(vnb, T, ar):
+        # the launch shape of the plain path for (dim, precision, arithmetic), timed on this
+        # grid once (untimed here) and cached on the machine
+        if args.no_tune:
+            return None
+        from hydro_b200.autotune import tune_plain
+
+        key = f"{len(vnb)}d_{np.dtype(T).name}_{ar}"
+        if key not in tuned:
+            tuned[key] = tune_plain(vnb, T, ar, log=log)
+        hb.set_launch_shape(len(vnb), T, tuned[key]["warps"], tuned[key]["chunk"])
+        return tuned[key]
+
+    tune(nb, Tcase, args.arith)
     barrier()
     uuid = gpu_uuid(torch, local)
     meter = EnergyMeter(uuid)
@@ -758,7 +848,8 @@ def main():
     kern_ms = statistics.mean(r["kernel_ms"])
     achieved = cells * bpc / (kern_ms / 1e3) / 1e9
     roofline = dict(bound="hbm", achieved=achieved, peak=hbm, unit="GB/s", frac=achieved / hbm,
-                    peak_kind=peak_kind, traffic=None, kernel=kname, bytes_per_cell=bpc, kernel_ms=kern_ms)
+                    peak_kind=peak_kind, traffic=None, kernel=kname, bytes_per_cell=bpc, kernel_ms=kern_ms,
+                    arith=args.arith, launch_shape=r["shape"])
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
         tr = json.loads(tp.read_text()).get(f"{kname}_dram_bytes_per_cell")
@@ -786,6 +877,7 @@ def main():
                                  ("3d_f64_512^3_fused", n3, np.float64, "fused"),
                                  ("3d_f32_512^3_strict", n3, np.float32, "strict"),
                                  ("3d_f32_512^3_fused", n3, np.float32, "fused")):
+            tune(vnb, T, ar)
             barrier()
             vsampler = ClockSampler(uuid)
             vsampler.start()
@@ -799,7 +891,8 @@ def main():
             vbpc = BYTES_PER_CELL[(len(vnb), np.dtype(T).itemsize)]
             variants[name] = dict(value=world * vc * nst / (vms / 1e3) / 1e9, unit=UNIT,
                                   kernel_gbs=vc * vbpc / (km / 1e3) / 1e9, frac=vc * vbpc / (km / 1e3) / 1e9 / hbm,
-                                  kernel=int(vr["kernel"]), ms_per_step=vms / nst, clocks=vclocks)
+                                  kernel=int(vr["kernel"]), ms_per_step=vms / nst, clocks=vclocks,
+                                  launch_shape=vr["shape"])
 
     accuracy = {}
     if rank == 0 and world == 1 and not args.no_accuracy and args.case == "2d_f64":
@@ -807,7 +900,6 @@ def main():
         for name, vnb in (("2d_40000x20000", nb), ("3d_512^3", (512, 512, 512))):
             accuracy[name] = accuracy_vs_strict_fp64(hb, torch, vnb, steps=args.accuracy_steps)
 
-    log = lambda msg: print(msg, file=sys.stderr, flush=True)
     batched = serving = None
     if rank == 0 and world == 1 and not args.no_batched and args.case == "2d_f64":
         barrier()
@@ -851,6 +943,8 @@ def main():
             line["variants_frac"] = {k: v["frac"] for k, v in variants.items()}
         if accuracy:
             line["accuracy_vs_strict_fp64"] = accuracy
+        if tuned:
+            line["autotuned_shapes"] = {k: dict(warps=v["warps"], chunk=v["chunk"]) for k, v in tuned.items()}
         line["energy"] = energy_entry(r["energy_j"], total_ms / 1e3, cells * args.steps)
         line["variants"] = variants
         line["batched"] = batched

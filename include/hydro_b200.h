@@ -194,6 +194,18 @@ int hydro2d_noalloc_last_info(void *stream, hydro_step_info_t *info);
 unsigned hydro2d_noalloc_launch_shape(size_t NB_X, size_t NB_Y, int strip, int sms, int *chunk, unsigned *grid_x,
                                       unsigned *grid_y);
 
+/* Launch shape of the plain strip kernels for (dim 2 or 3, precision 4 or 8 bytes), as an
+ * autotuner picks it: `warps` = warps per block of the 3D kernel, i.e. tile rows with the
+ * halo (8, 16, and 12 in FP64; 0 = built-in: 8 in FP64, 16 in FP32; must be 0 in 2D), and
+ * `chunk` = rows (2D) or planes (3D) each block marches (0 = sized from the grid and the
+ * SM count). Process-wide; the results do not depend on the shape. No counterpart in the
+ * reference, whose single-task kernel has no launch shape. */
+int hydro_set_launch_shape(int dim, int precision_bytes, int warps, int chunk);
+/* The shape the last strip-kernel step on the current device used: warps per block (0 in
+ * 2D), rows or planes per block, and whether its rows / planes were staged by tensor-map
+ * loads (1) or per-lane copies (0). */
+int hydro_last_launch_shape(int *warps, int *chunk, int *tma);
+
 /* Diagnostics: the number of per-device contexts (scratch words, partial sums, a pinned
  * status record) the regular entry points have created in this process. The
  * allocation-free entry points create none. No counterpart in the reference. */

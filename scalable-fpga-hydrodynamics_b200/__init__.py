@@ -99,6 +99,10 @@ def _declare(lib):
         fn = getattr(lib, f"hydro_mass_{suf}")
         fn.argtypes = [_vp, _c_size, _c_size, _c_size, pd, _vp]
         fn.restype = ctypes.c_int
+    lib.hydro_set_launch_shape.argtypes = [ctypes.c_int] * 4
+    lib.hydro_set_launch_shape.restype = ctypes.c_int
+    lib.hydro_last_launch_shape.argtypes = [ctypes.POINTER(ctypes.c_int)] * 3
+    lib.hydro_last_launch_shape.restype = ctypes.c_int
     lib.hydro_last_step_info.argtypes = [ctypes.POINTER(StepInfo)]
     lib.hydro_last_step_info.restype = ctypes.c_int
     lib.hydro_last_error.restype = ctypes.c_int
@@ -116,6 +120,20 @@ def lib():
             raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}`")
         _lib = _declare(ctypes.CDLL(str(LIB_PATH)))
     return _lib
+
+
+def set_launch_shape(dim: int, dtype, warps: int = 0, chunk: int = 0):
+    """Launch shape of the plain strip kernels for (dim, precision): 3D warps per block
+    (tile rows with halo; 0 = built-in) and rows / planes per block (0 = sized from the
+    grid). Results do not depend on it."""
+    _check(lib().hydro_set_launch_shape(int(dim), np.dtype(dtype).itemsize, int(warps), int(chunk)))
+
+
+def last_launch_shape() -> dict:
+    """The shape the last strip-kernel step on the current device used."""
+    w, c, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().hydro_last_launch_shape(ctypes.byref(w), ctypes.byref(c), ctypes.byref(t)))
+    return dict(warps=w.value, chunk=c.value, tma=bool(t.value))
 
 
 def last_error() -> tuple[int, str]:

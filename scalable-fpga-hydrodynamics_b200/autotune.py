@@ -1,13 +1,23 @@
-"""Tile-shape autotuner for the batched step, keyed on dimensionality and precision.
+"""Tile-shape autotuner, keyed on dimensionality and precision.
 
-The batched kernels take a fixed block shape (2D: 128 lanes over 126 interior columns;
-3D: 8 x 32 lanes over 6 x 30 interior columns in FP64, 16 x 32 over 14 x 30 in FP32) and
-one free tile parameter: the number
-of X rows (planes) a work item marches, `chunk`. Longer chunks re-read fewer halo rows
-and take fewer work items; shorter ones balance uneven instances better. `tune` times a
-seeded mini-batch of the batched workload for each candidate and keeps the fastest;
-results are cached per (GPU name, dimensionality, precision) in a JSON file next to this
-module (written on the machine that runs it, not shipped).
+Plain path (`tune_plain`): the strip kernels take two shape parameters, the tile height of
+the 3D kernel (warps per block, i.e. tile rows with the one-row halo: 8, 12 or 16 in FP64,
+8 or 16 in FP32) and the number of X rows (2D) or planes (3D) each block marches (`chunk`,
+or 0 for the built-in size from the grid and the SM count). Taller tiles recompute fewer
+halo rows but hold one block per SM; longer chunks re-read fewer halo rows but give fewer
+blocks. `tune_plain` times a few steps of the blast on the grid it is given for every
+candidate (warps x chunk), keeps the fastest and installs it in the library
+(hydro_set_launch_shape); the results do not depend on the shape.
+
+Batched path (`tune`): the batched kernels take a fixed block shape (2D: 128 lanes over
+126 interior columns; 3D: 8 x 32 lanes over 6 x 30 interior columns in FP64, 16 x 32 over
+14 x 30 in FP32) and one free tile parameter, the rows (planes) a work item marches,
+`chunk`. Longer chunks re-read fewer halo rows and take fewer work items; shorter ones
+balance uneven instances better. `tune` times a seeded mini-batch of the batched
+workload for each candidate and keeps the fastest.
+
+Results are cached per (GPU name, dimensionality, precision[, arithmetic]) in a JSON file
+next to this module (written on the machine that runs it, not shipped).
 """
 from __future__ import annotations
 
@@ -18,7 +28,7 @@ from pathlib import Path
 
 import numpy as np
 
-from . import _torch
+from . import BlastRun, _torch, last_launch_shape, set_launch_shape
 from .batch import Batch
 from .workloads import batch_blasts
 
@@ -95,3 +105,60 @@ def best_chunk(dim, dtype):
     """The tuned chunk if known on this machine, else the engine default (0)."""
     entry = _load().get(_key(dim, dtype))
     return int(entry["chunk"]) if entry else 0
+
+
+# plain-path candidates: 3D tile heights (warps per block) per precision, and chunks
+PLAIN_WARPS = {(2, 4): (0,), (2, 8): (0,), (3, 4): (8, 16), (3, 8): (8, 12, 16)}
+PLAIN_CHUNKS = {2: (0, 32, 64, 128, 256), 3: (0, 16, 32, 64, 128)}
+
+
+def measure_plain(nb, dtype, arith, warps, chunk, steps=4, warmup=2):
+    """Cell-updates per second of the plain path with one launch shape (CUDA events around
+    `steps` steps after `warmup`), on the blast of grid `nb`."""
+    torch = _torch()
+    dim = len(nb)
+    set_launch_shape(dim, dtype, warps, chunk)
+    run = BlastRun(nb, dtype, arith=arith)
+    for _ in range(warmup):
+        run.step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        run.step()
+    e1.record()
+    torch.cuda.synchronize()
+    shape = last_launch_shape()
+    del run
+    torch.cuda.empty_cache()
+    return int(np.prod(nb)) * steps / (e0.elapsed_time(e1) / 1e3), shape
+
+
+def tune_plain(nb, dtype, arith="strict", force=False, log=None):
+    """The fastest (warps, chunk) of the plain path for (this GPU, dim, dtype, arith), timed
+    on grid `nb` once and then cached; installs it and returns it as a dict."""
+    dim = len(nb)
+    T = np.dtype(dtype)
+    cache = _load()
+    key = f"plain|{_key(dim, dtype)}|{arith}"
+    if key in cache and not force:
+        best = cache[key]
+        set_launch_shape(dim, dtype, best["warps"], best["chunk"])
+        return best
+    results = []
+    for w in PLAIN_WARPS[(dim, T.itemsize)]:
+        for c in PLAIN_CHUNKS[dim]:
+            rate, shape = measure_plain(nb, dtype, arith, w, c)
+            results.append((rate, w, c, shape))
+            if log:
+                log(f"autotune {key} warps {w} chunk {c}: {rate / 1e9:.1f} GCell/s (ran {shape})")
+    rate, w, c, shape = max(results, key=lambda r: r[0])
+    best = dict(warps=w, chunk=c, gcell_s=rate / 1e9, grid=list(nb), ran=shape,
+                tried={f"{r[1]}x{r[2]}": r[0] / 1e9 for r in results})
+    cache[key] = best
+    try:
+        CACHE.write_text(json.dumps(cache, indent=1))
+    except OSError:
+        pass
+    set_launch_shape(dim, dtype, w, c)
+    return best

@@ -297,6 +297,22 @@ int hydro_last_step_info(hydro_step_info_t *info)
 
 int hydro_device_contexts(void) { return ctx_count(); }
 
+int hydro_set_launch_shape(int dim, int precision_bytes, int warps, int chunk)
+{
+    return set_launch_shape(dim, (size_t)precision_bytes, warps, chunk);
+}
+
+int hydro_last_launch_shape(int *warps, int *chunk, int *tma)
+{
+    int err;
+    DevCtx *c = ctx_current(&err);
+    if (!c) return err;
+    if (warps) *warps = c->last_warps;
+    if (chunk) *chunk = c->last_chunk;
+    if (tma) *tma = c->last_tma ? 1 : 0;
+    return kOk;
+}
+
 int hydro_last_error(void) { return last_error(); }
 const char *hydro_last_error_string(void) { return last_error_string(); }
 void hydro_clear_error(void) { clear_error(); }

@@ -96,6 +96,30 @@ int device_sms()
     return n;
 }
 
+namespace {
+LaunchShape g_shape[2][2]; // [dim - 2][FP64]
+} // namespace
+
+LaunchShape launch_shape(int dim, size_t tsize)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_shape[dim == 3][tsize == 8];
+}
+
+int set_launch_shape(int dim, size_t tsize, int warps, int chunk)
+{
+    if ((dim != 2 && dim != 3) || (tsize != 4 && tsize != 8) || chunk < 0 || chunk > (1 << 20) ||
+        (dim == 2 && warps != 0) ||
+        (dim == 3 && warps != 0 && warps != 8 && warps != 16 && !(tsize == 8 && warps == 12))) {
+        set_error(kErrArg, "hydro_set_launch_shape: unsupported shape (dim %d, %zu-byte values, %d warps, chunk %d)",
+                  dim, tsize, warps, chunk);
+        return kErrArg;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_shape[dim == 3][tsize == 8] = LaunchShape{warps, chunk};
+    return kOk;
+}
+
 int ctx_count()
 {
     std::lock_guard<std::mutex> lk(g_mu);

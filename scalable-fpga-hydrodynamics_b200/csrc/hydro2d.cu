@@ -352,10 +352,18 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
     unsigned nblocks;
     if (use_strip) {
         const int nstrips = (int)((nb_y + kStripW - 1) / kStripW);
-        const int target = device_sms() * 3 * 8;
-        int nchunks = (target + nstrips - 1) / nstrips;
-        int chunk = (int)((nb_x + nchunks - 1) / nchunks);
-        chunk = std::min(256, std::max(16, chunk));
+        // rows per block: the tuned value when one is set (hydro_set_launch_shape), else
+        // sized for about 24 blocks per SM
+        const LaunchShape shape = launch_shape(2, sizeof(T));
+        int nchunks, chunk;
+        if (shape.chunk > 0) {
+            chunk = shape.chunk;
+        } else {
+            const int target = device_sms() * 3 * 8;
+            nchunks = (target + nstrips - 1) / nstrips;
+            chunk = (int)((nb_x + nchunks - 1) / nchunks);
+            chunk = std::min(256, std::max(16, chunk));
+        }
         nchunks = (int)((nb_x + chunk - 1) / chunk);
         if (nchunks > 65535) {
             chunk = (int)((nb_x + 65534) / 65535);
@@ -365,6 +373,9 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
         nblocks = (unsigned)nstrips * (unsigned)nchunks;
         if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
         g.partials = ctx->partials;
+        ctx->last_warps = 0;
+        ctx->last_chunk = chunk;
+        ctx->last_tma = tma_ok;
         const dim3 grid(nstrips, nchunks);
         if (tma_ok && fused)
             strip2d<T, true, true><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);

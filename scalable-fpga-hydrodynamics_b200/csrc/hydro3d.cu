@@ -108,13 +108,13 @@ template <class T, bool kF = false> __global__ void __launch_bounds__(k3RedoNT) 
 
 // ------------------------------------------------------------------- strip kernel ---
 // kF: fused arithmetic (hydro_math.cuh). kTma: planes staged by the tensor maps tmr/tmu
-// (FP64, even NB_Z), else by per-lane cp.async.
-template <class T, bool kF, bool kTma>
-__global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>)
+// (FP64, even NB_Z), else by per-lane cp.async. W: warps per block (tile rows with halo).
+template <class T, bool kF, bool kTma, int W>
+__global__ void __launch_bounds__(32 * W, min_blocks3(W))
     strip3d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args3<T> g)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    Smem3<T> &S = *reinterpret_cast<Smem3<T> *>(smem_raw);
+    Smem3<T, W> &S = *reinterpret_cast<Smem3<T, W> *>(smem_raw);
     if constexpr (kTma) {
         if (threadIdx.x == 0) {
             prefetch_tensormap(&tmr);
@@ -123,13 +123,13 @@ __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>)
         march3d_init(S);
     }
     const int i0 = 1 + g.chunk * (int)blockIdx.z;
-    const March3 geo{k3TZ * (int)blockIdx.x, k3TY<T> * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
+    const March3 geo{k3TZ * (int)blockIdx.x, (W - 2) * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
                      g.nb_x, g.nb_y, g.nb_z, g.zs, g.zy, g.xwrap};
     StepAcc acc;
     const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
     const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
     const Phys<T> ph = g.ph;
-    const bool ok = march3d<T, kF, kTma>(
+    const bool ok = march3d<T, kF, kTma, W>(
         S, g.rhoE, g.uvw, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz,
         [&](const Upd3<T> &o) {
             acc.add_mass(o.r);
@@ -139,9 +139,33 @@ __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>)
         },
         Tmaps3{&tmr, &tmu});
     if (!ok) acc.err |= kErrWaitTimeout;
-    step_epilogue<k3NT<T>, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
-                           blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
-                           g.status, g.seq, (double)tlof, g.key);
+    step_epilogue<32 * W, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
+                             blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
+                             g.status, g.seq, (double)tlof, g.key);
+}
+
+// Tile heights the plain 3D step is built for: FP64 8 (default), 12 and 16 warps; FP32 8
+// and 16 (default). The tensor-map staging is built for FP64 only.
+template <class T> constexpr bool tile3_built(int W)
+{
+    return sizeof(T) == 8 ? (W == 8 || W == 12 || W == 16) : (W == 8 || W == 16);
+}
+
+template <class T, int W>
+cudaError_t launch_strip3d(bool fused, bool tma, dim3 grid, cudaStream_t stream, const CUtensorMap &tmr,
+                           const CUtensorMap &tmu, const Args3<T> &g)
+{
+    void (*kern)(const CUtensorMap, const CUtensorMap, Args3<T>);
+    if constexpr (sizeof(T) == 8)
+        kern = fused ? (tma ? strip3d<T, true, true, W> : strip3d<T, true, false, W>)
+                     : (tma ? strip3d<T, false, true, W> : strip3d<T, false, false, W>);
+    else
+        kern = fused ? strip3d<T, true, false, W> : strip3d<T, false, false, W>;
+    const int smem = (int)sizeof(Smem3<T, W>);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, 32 * W, smem, stream>>>(tmr, tmu, g);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------- initial condition ---
@@ -261,15 +285,24 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
     const bool use_strip = which != Kernel::Direct;
     unsigned nblocks;
     if (use_strip) {
-        const int nz = (int)((nb_z + k3TZ - 1) / k3TZ), ny = (int)((nb_y + k3TY<T> - 1) / k3TY<T>);
+        // tile height and planes per block: the tuned shape when one is set
+        // (hydro_set_launch_shape), else the built-in one
+        const LaunchShape shape = launch_shape(3, sizeof(T));
+        const int W = (shape.warps > 0 && tile3_built<T>(shape.warps)) ? shape.warps : k3Warps<T>;
+        const int nz = (int)((nb_z + k3TZ - 1) / k3TZ), ny = (int)((nb_y + (W - 2) - 1) / (W - 2));
         if (ny > 65535) {
             set_error(kErrArg, "step3d: NB_Y %zu too large for the strip kernel", nb_y);
             return kErrArg;
         }
-        const int target = device_sms() * 2 * 8;
-        int nchunks = std::max(1, (target + nz * ny - 1) / (nz * ny));
-        int chunk = (int)((nb_x + nchunks - 1) / nchunks);
-        chunk = std::min(256, std::max(8, chunk));
+        int nchunks, chunk;
+        if (shape.chunk > 0) {
+            chunk = shape.chunk;
+        } else {
+            const int target = device_sms() * min_blocks3(W) * 8;
+            nchunks = std::max(1, (target + nz * ny - 1) / (nz * ny));
+            chunk = (int)((nb_x + nchunks - 1) / nchunks);
+            chunk = std::min(256, std::max(8, chunk));
+        }
         nchunks = (int)((nb_x + chunk - 1) / chunk);
         if (nchunks > 65535) {
             chunk = (int)((nb_x + 65534) / 65535);
@@ -289,19 +322,30 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         if (tma) {
             const uint64_t zs = nb_z + 2, ys = nb_y + 2, xs = nb_x + 2;
             tma = encode_tmap_3d(&tmr, tmap_type3<T>(), rhoE, 2 * zs, ys, xs, 2 * zs * sizeof(T), 2 * zs * ys * sizeof(T),
-                                 64, k3Warps<T>, 1) &&
+                                 64, (uint32_t)W, 1) &&
                   encode_tmap_3d(&tmu, tmap_type3<T>(), uvw, 3 * zs, ys, xs, 3 * zs * sizeof(T), 3 * zs * ys * sizeof(T),
-                                 96, k3Warps<T>, 1);
+                                 96, (uint32_t)W, 1);
         }
-        auto kern = fused ? (tma ? strip3d<T, true, true> : strip3d<T, true, false>)
-                          : (tma ? strip3d<T, false, true> : strip3d<T, false, false>);
-        const int smem = (int)sizeof(Smem3<T>);
-        cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        const dim3 grid(nz, ny, nchunks);
+        cudaError_t ea;
+        if (W == 8) {
+            ea = launch_strip3d<T, 8>(fused, tma, grid, stream, tmr, tmu, g);
+        } else if constexpr (sizeof(T) == 8) {
+            if (W == 12)
+                ea = launch_strip3d<T, 12>(fused, tma, grid, stream, tmr, tmu, g);
+            else
+                ea = launch_strip3d<T, 16>(fused, tma, grid, stream, tmr, tmu, g);
+        } else {
+            ea = launch_strip3d<T, 16>(fused, tma, grid, stream, tmr, tmu, g);
+        }
         if (ea != cudaSuccess) {
-            set_error(kErrCuda, "step3d: shared-memory attribute: %s", cudaGetErrorString(ea));
+            ctx->dirty = true;
+            set_error(kErrCuda, "step3d launch: %s", cudaGetErrorString(ea));
             return kErrCuda;
         }
-        kern<<<dim3(nz, ny, nchunks), k3NT<T>, smem, stream>>>(tmr, tmu, g);
+        ctx->last_warps = W;
+        ctx->last_chunk = chunk;
+        ctx->last_tma = tma;
     } else {
         const int gx = (int)((nb_z + 31) / 32), gy = (int)((nb_y + 3) / 4), gz = (int)std::min<size_t>(nb_x, 65535);
         if (gy > 65535) {

@@ -28,6 +28,9 @@ struct DevCtx {
     StepStatus *status_d = nullptr; // device alias of status_h
     unsigned seq = 0;
     int last_kernel = 0; // Kernel run by the last step launch
+    int last_warps = 0;  // its launch shape (strip kernels): warps per block, rows/planes per block
+    int last_chunk = 0;
+    bool last_tma = false; // its rows/planes staged by tensor-map loads
     bool dirty = false; // a launch failed: scratch words must be re-zeroed
 };
 
@@ -67,6 +70,15 @@ inline unsigned long long problem_key(const void *dt_next, size_t a, size_t b, s
     k ^= tsize << 56;
     return k ? k : 1ull;
 }
+
+// Launch shape of the plain strip kernels per (dimensionality, precision), set by
+// hydro_set_launch_shape (an autotuner); 0 fields keep the built-in choice.
+struct LaunchShape {
+    int warps = 0; // 3D: warps per block (tile rows with halo)
+    int chunk = 0; // rows (2D) or planes (3D) each block marches
+};
+LaunchShape launch_shape(int dim, size_t tsize);
+int set_launch_shape(int dim, size_t tsize, int warps, int chunk);
 
 // Context of the current device (created on first use; never freed before exit).
 DevCtx *ctx_current(int *err);

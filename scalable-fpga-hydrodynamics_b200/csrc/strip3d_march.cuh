@@ -27,10 +27,13 @@ namespace hydro {
 // per SM), FP64 8 warps (6 interior rows; two 256-thread blocks per SM, the most its
 // 128-register budget allows). Measured at 512^3: FP32 48.3 -> 50.1 GCell/s with 16 warps,
 // FP64 31.5 -> 28.4 (it spills and loses the second block).
+// The plain step also takes other tile heights (warps W per block, W - 2 interior rows),
+// chosen at run time (hydro_set_launch_shape): k3Warps is the default.
 template <class T> constexpr int k3Warps = sizeof(T) == 4 ? 16 : 8; // y extent of the tile (with halo)
 template <class T> constexpr int k3NT = 32 * k3Warps<T>;             // threads
 template <class T> constexpr int k3TY = k3Warps<T> - 2;              // interior rows per tile
 template <class T> constexpr int k3MinBlocks = k3Warps<T> <= 8 ? 2 : 1; // resident blocks per SM
+constexpr int min_blocks3(int W) { return W <= 8 ? 2 : 1; }
 constexpr int k3TZ = 30;           // interior columns per tile
 constexpr int k3Stages = 4;
 
@@ -44,34 +47,34 @@ template <class T> __device__ __forceinline__ typename Vec2<T>::type pair3(T a, 
     return v;
 }
 
-template <class T> struct Smem3 {
+template <class T, int W = k3Warps<T>> struct Smem3 {
     using V2 = typename Vec2<T>::type;
+    static constexpr int NT = 32 * W;
     union {
-        T st[k3Stages][5][k3NT<T>]; // per-lane copies, per plane: rho, E, rho_u, rho_v, rho_w
-        struct {                    // tensor-map boxes in tile order (lane t = 32 row + column)
-            T r[k3Stages][k3NT<T>][2]; // (rho, E)
-            T u[k3Stages][k3NT<T>][3]; // (rho u, rho v, rho w)
+        T st[k3Stages][5][NT]; // per-lane copies, per plane: rho, E, rho_u, rho_v, rho_w
+        struct {               // tensor-map boxes in tile order (lane t = 32 row + column)
+            T r[k3Stages][NT][2]; // (rho, E)
+            T u[k3Stages][NT][3]; // (rho u, rho v, rho w)
         } tm;
     };
     uint64_t full[k3Stages]; // tensor-map form: stage s holds its plane
     int abort;
     // each lane's cell by plane parity, as pairs (r,p) (Ka,iKa) (v,w) (mu,mv) (mw,eup_xy)
     // (eup_z,-): the warp below reads its y-face inputs, the previous lane its z-face inputs
-    V2 xP[2][6][k3NT<T>];
-    V2 xF[2][2][k3NT<T>]; // each lane's +y face flux by plane parity: (r,n) (t1,t2) ...
-    T xFE[2][k3NT<T>];    // ... and E
+    V2 xP[2][6][NT];
+    V2 xF[2][2][NT]; // each lane's +y face flux by plane parity: (r,n) (t1,t2) ...
+    T xFE[2][NT];    // ... and E
 };
 
-// a neighbour's face inputs from the exchange buffer (layout of Smem3::xP)
-template <class T> __device__ __forceinline__ FaceIn3<T> xp_face_y(const typename Vec2<T>::type *x)
+// a neighbour's face inputs from the exchange buffer (layout of Smem3::xP, NT lanes)
+template <class T, int NT> __device__ __forceinline__ FaceIn3<T> xp_face_y(const typename Vec2<T>::type *x)
 {
-    const auto q0 = x[0 * k3NT<T>], q1 = x[1 * k3NT<T>], q2 = x[2 * k3NT<T>], q3 = x[3 * k3NT<T>], q4 = x[4 * k3NT<T>];
+    const auto q0 = x[0 * NT], q1 = x[1 * NT], q2 = x[2 * NT], q3 = x[3 * NT], q4 = x[4 * NT];
     return FaceIn3<T>{q0.x, q2.x, q0.y, q1.x, q1.y, q3.y, q3.x, q4.x, q4.y}; // normal v: (v, u, w)
 }
-template <class T> __device__ __forceinline__ FaceIn3<T> xp_face_z(const typename Vec2<T>::type *x)
+template <class T, int NT> __device__ __forceinline__ FaceIn3<T> xp_face_z(const typename Vec2<T>::type *x)
 {
-    const auto q0 = x[0 * k3NT<T>], q1 = x[1 * k3NT<T>], q2 = x[2 * k3NT<T>], q3 = x[3 * k3NT<T>], q4 = x[4 * k3NT<T>],
-               q5 = x[5 * k3NT<T>];
+    const auto q0 = x[0 * NT], q1 = x[1 * NT], q2 = x[2 * NT], q3 = x[3 * NT], q4 = x[4 * NT], q5 = x[5 * NT];
     return FaceIn3<T>{q0.x, q2.y, q0.y, q1.x, q1.y, q4.x, q3.y, q3.x, q5.x}; // normal w: (w, v, u)
 }
 
@@ -92,7 +95,7 @@ struct Tmaps3 {
 
 // One-time set-up of the stage barriers of the tensor-map form (thread 0), then a block
 // barrier.
-template <class T> __device__ __forceinline__ void march3d_init(Smem3<T> &S)
+template <class T, int W> __device__ __forceinline__ void march3d_init(Smem3<T, W> &S)
 {
     if (threadIdx.x == 0) {
         for (int s = 0; s < k3Stages; ++s) mbar_init(&S.full[s], 1);
@@ -103,8 +106,8 @@ template <class T> __device__ __forceinline__ void march3d_init(Smem3<T> &S)
 }
 
 // Returns false when a bounded barrier wait of the tensor-map form gave up.
-template <bool kEdge, bool kF, bool kTma, class T, class Sink>
-__device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
+template <bool kEdge, bool kF, bool kTma, class T, int W, class Sink>
+__device__ __forceinline__ bool march3d_tile(Smem3<T, W> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
                                              const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz,
                                              const Tmaps3 &tm, Sink &sink)
 {
@@ -113,8 +116,8 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T
     const int k = g.kbase + lane, j = g.jbase + w;
     const int nplanes = g.i1 - g.i0 + 3;
     const bool interior =
-        (w >= 1) && (w <= k3TY<T>) && (lane >= 1) && (lane <= k3TZ) && (!kEdge || ((j <= g.nb_y) && (k <= g.nb_z)));
-    const bool iwarp = (w >= 1) && (w <= k3TY<T>) && (!kEdge || (g.jbase + 1 <= g.nb_y)); // warp holds interior rows
+        (w >= 1) && (w <= (W - 2)) && (lane >= 1) && (lane <= k3TZ) && (!kEdge || ((j <= g.nb_y) && (k <= g.nb_z)));
+    const bool iwarp = (w >= 1) && (w <= (W - 2)) && (!kEdge || (g.jbase + 1 <= g.nb_y)); // warp holds interior rows
     const long long colofs = (long long)j * g.zs + k;
     // ghost cells (j or k = 0 or NB+1) and cells past the array are never used: they
     // convert a unit state so every lane's reciprocal / square root stays regular
@@ -124,7 +127,6 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T
     // lane its column k). FP64 tiles: every lane copies its own cell. Measured at 512^3:
     // FP32 49.8 -> 50.7-52.3 GCell/s with the halo warps loading, FP64 31.6 -> 30.9, so
     // each precision keeps the faster form. Cells past the array load as zeros.
-    constexpr int W = k3Warps<T>;
     constexpr bool kHaloLoads = sizeof(T) == 4;
     const bool loader = kHaloLoads ? ((w == 0) || (w == W - 1)) : true;
     const int rbase = kHaloLoads ? ((w == 0) ? 0 : W / 2) : w;
@@ -132,7 +134,7 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T
     const bool kin = !kEdge || (k <= g.nb_z + 1);
 
     __syncthreads(); // the previous march of this block is done with the stages and exchange buffers
-    constexpr uint32_t kPlaneBytes = (uint32_t)(5 * k3NT<T> * sizeof(T));
+    constexpr uint32_t kPlaneBytes = (uint32_t)(5 * (32 * W) * sizeof(T));
     // tensor-map form: thread 0 loads plane m into stage m % k3Stages (a single march per
     // block: stage s completes its phase (m / k3Stages) & 1)
     auto issue_tma = [&](int m) {
@@ -194,7 +196,7 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T
         if constexpr (kTma) {
             if (t == 0 && m + k3Stages - 1 < nplanes) issue_tma(m + k3Stages - 1);
             if (!mbar_wait_bounded(&S.full[s], (uint32_t)(m / k3Stages) & 1u)) S.abort = 1;
-            const typename Smem3<T>::V2 a = *reinterpret_cast<const typename Smem3<T>::V2 *>(&S.tm.r[s][t][0]);
+            const typename Smem3<T, W>::V2 a = *reinterpret_cast<const typename Smem3<T, W>::V2 *>(&S.tm.r[s][t][0]);
             ur = a.x;
             uE = a.y;
             uu = S.tm.u[s][t][0];
@@ -220,18 +222,18 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T
         }
         const Cell3<T> P = make_cell3<T, kF>(ur, uu, uv, uw, uE, ph);
         {
-            typename Smem3<T>::V2 *x = &S.xP[m & 1][0][t];
-            x[0 * k3NT<T>] = pair3<T>(P.r, P.p);
-            x[1 * k3NT<T>] = pair3<T>(P.Ka, P.iKa);
-            x[2 * k3NT<T>] = pair3<T>(P.v, P.w);
-            x[3 * k3NT<T>] = pair3<T>(P.mu, P.mv);
-            x[4 * k3NT<T>] = pair3<T>(P.mw, P.eup_xy);
-            x[5 * k3NT<T>] = pair3<T>(P.eup_z, T(0));
+            typename Smem3<T, W>::V2 *x = &S.xP[m & 1][0][t];
+            x[0 * (32 * W)] = pair3<T>(P.r, P.p);
+            x[1 * (32 * W)] = pair3<T>(P.Ka, P.iKa);
+            x[2 * (32 * W)] = pair3<T>(P.v, P.w);
+            x[3 * (32 * W)] = pair3<T>(P.mu, P.mv);
+            x[4 * (32 * W)] = pair3<T>(P.mw, P.eup_xy);
+            x[5 * (32 * W)] = pair3<T>(P.eup_z, T(0));
         }
         // +y face of (j | j+1), from this lane's previous-plane cell and the warp above's
         auto yface = [&]() {
             const FaceIn3<T> me = face3_y(Pm);
-            const FaceIn3<T> nb = xp_face_y<T>(&S.xP[(m - 1) & 1][0][t + 32]);
+            const FaceIn3<T> nb = xp_face_y<T, 32 * W>(&S.xP[(m - 1) & 1][0][t + 32]);
             FaceIn3<T> L = me, R = nb;
             if (kEdge) {
                 if (j == 0) L = mirror3(nb);
@@ -243,7 +245,7 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T
         // reads the next warp's lane 0, a face no interior lane uses)
         auto zface = [&]() {
             const FaceIn3<T> mz = face3_z(Pm);
-            const FaceIn3<T> nz = xp_face_z<T>(&S.xP[(m - 1) & 1][0][t + 1]);
+            const FaceIn3<T> nz = xp_face_z<T, 32 * W>(&S.xP[(m - 1) & 1][0][t + 1]);
             FaceIn3<T> L = mz, R = nz;
             if (kEdge) {
                 if (k == 0) L = mirror3(nz);
@@ -267,7 +269,7 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T
                 fy = yface();
                 fz = zface();
                 publish_y(fy);
-            } else if (w < k3Warps<T> - 1) {
+            } else if (w < W - 1) {
                 fy = yface();
                 publish_y(fy);
             }
@@ -323,13 +325,12 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T> &S, const T *rhoE, const T
 // elsewhere (the choice is uniform over the block). kF: fused arithmetic (hydro_math.cuh).
 // kTma: planes staged by the tensor maps `tm` (march3d_init first); else per-lane copies.
 // Returns false when a bounded barrier wait gave up.
-template <class T, bool kF = false, bool kTma = false, class Sink>
-__device__ __forceinline__ bool march3d(Smem3<T> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
+template <class T, bool kF = false, bool kTma = false, int W = k3Warps<T>, class Sink>
+__device__ __forceinline__ bool march3d(Smem3<T, W> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
                                         const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &&sink,
                                         const Tmaps3 &tm = Tmaps3{})
 {
-    const bool inner =
-        g.jbase >= 1 && g.jbase + k3Warps<T> - 1 <= g.nb_y && g.kbase >= 1 && g.kbase + 31 <= g.nb_z;
+    const bool inner = g.jbase >= 1 && g.jbase + W - 1 <= g.nb_y && g.kbase >= 1 && g.kbase + 31 <= g.nb_z;
     if (inner) return march3d_tile<false, kF, kTma>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, tm, sink);
     return march3d_tile<true, kF, kTma>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, tm, sink);
 }

@@ -65,6 +65,7 @@ class Server:
         self.capacity = capacity
         self.engines = {}
         self.streams = {}
+        self.stats = {}
 
     def engine(self, dim, dtype) -> Batch:
         key = (dim, np.dtype(dtype).name)
@@ -91,6 +92,9 @@ class Server:
         active = {}  # (key, slot) -> (request, bytes)
         used = 0.0
         nxt = 0
+        # budget statistics: the most bytes held at once, the longest queue of arrived
+        # requests waiting, and the ticks on which a waiting request did not fit
+        self.stats = dict(budget_bytes=self.budget, peak_bytes=0.0, max_waiting=0, ticks_budget_bound=0, ticks=0)
         t0 = time.perf_counter()
         clock = lambda: time.perf_counter() - t0
         while True:
@@ -114,12 +118,17 @@ class Server:
                 active[((len(r.blast.nb), np.dtype(prec(r)).name), slot)] = (r, need)
                 recs[r.rid].admit = clock()
                 pending.popleft()
+            self.stats["peak_bytes"] = max(self.stats["peak_bytes"], used)
+            self.stats["max_waiting"] = max(self.stats["max_waiting"], len(pending))
+            if pending:
+                self.stats["ticks_budget_bound"] += 1
             if not active:
                 if nxt >= len(reqs) and not pending:
                     break
                 if nxt < len(reqs):
                     time.sleep(max(0.0, min(0.002, reqs[nxt].arrival - clock())))
                 continue
+            self.stats["ticks"] += 1
             busy = {k for (k, _s) in active}
             for k in busy:
                 self.engines[k].run(self.steps_per_tick, sync=False)

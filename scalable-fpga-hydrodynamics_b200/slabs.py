@@ -1,22 +1,32 @@
 """The reference's X-slab decomposition over ranks (hydro2d/main.cxx:621-636, --sdx N
 --sdy 1; hydro3d likewise), one process per GPU.
 
-Rank r of N owns a contiguous range of global X rows (2D) or planes (3D). Every step:
-  1. each rank sends its first interior row to the rank on its left and its last to the
-     rank on its right, which store them in their ghost rows NB_X+1 and 0 (periodic across
-     ranks: rank 0's left neighbour is rank N-1), as the reference's host exchange does
-     (hydro2d/main.cxx:381-424);
-  2. each rank steps its slab with the X ghost rows read from memory (X_GHOSTS_FROM_MEMORY);
-  3. the next Dt is the MIN of the ranks' Dt (main.cxx:781) and t advances by it.
-The update of a cell depends only on its neighbours, so the state after n steps is
-bit-identical to the whole domain stepped on one device. The exchange is the only
-collective on the data path: two rows per rank per step, plus one scalar MIN.
+Rank r of N owns a contiguous range of global X rows (2D) or planes (3D). The update of a
+cell depends only on its neighbours, so the state after n steps is bit-identical to the
+whole domain stepped on one device. The exchange is the only collective on the data path:
+two rows per rank per step, plus one scalar MIN of Dt (main.cxx:781).
+
+Each step overlaps the exchange with the bulk of the update:
+  1. the two edge rows (1 and n) of the slab are updated first; they read the ghost rows 0
+     and n+1 that the previous step's exchange filled;
+  2. the new edge rows are sent to the neighbouring ranks (rank 0's left neighbour is rank
+     N-1), which receive them into the ghost rows of their new state, as the reference's
+     host exchange does (hydro2d/main.cxx:381-424), while
+  3. the interior rows 2 .. n-1 are updated (they read rows 1 .. n only);
+  4. the exchange is completed, the three partial Dt are combined (the minimum of
+     C_min / max over parts is C_min / the max over the slab: division by a positive
+     maximum is monotone) and the MIN over ranks is taken on the device; one scalar comes
+     back to the host for the next step's DtDx, as in the reference's loop.
+Every update of a part of the slab is one step call on a view of the state whose first row
+is the part's lower X neighbour, with the X neighbours read from memory.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
-from . import (KERNEL_AUTO, HydroError, Physics, _torch, alloc_state, init_blast_at, mass, step)
+from . import (KERNEL_AUTO, HydroError, Physics, StepInfo, _check, alloc_state, init_blast_at, lib, mass, step)
 from .batch import Blast
 from .replicas import Replicas
 
@@ -31,68 +41,116 @@ def slab_rows(nb_x: int, world: int, rank: int):
     return lo, lo + base + (1 if rank < extra else 0) - 1
 
 
+def _gpu_stepper(stream, kernel, arith):
+    """Step function of the GPU library: (state_in, state_out, dt_out, phys, dtd, sync)."""
+
+    def run(cur, nxt, dt_out, phys, dtd, sync):
+        _, info = step(cur, nxt, dt_out, phys, dtd, kernel=kernel, sync=sync, stream=stream, x_ghosts=True,
+                       arith=arith)
+        return info
+
+    return run
+
+
 class XSlabRun:
     """One rank's slab of the reference blast (2D or 3D), stepped in lock step with the
     other ranks of `reps` (Replicas: torch.distributed over NCCL on GPUs, or gloo, which
-    stages the exchanged rows through host memory)."""
+    stages the exchanged rows through host memory).
 
-    def __init__(self, nb, dtype, reps: Replicas, kernel=KERNEL_AUTO, stream=None):
-        torch = _torch()
+    `stepper` and `state` replace the GPU library for a run on the host (the schedule and
+    the exchange are the same): stepper(state_in, state_out, dt_out, phys, dtd, sync) steps
+    the rows of views whose first and last rows are X ghosts, and `state` gives the slab's
+    initial (rhoE, uvx) arrays (torch tensors with ghost rows) and first Dt."""
+
+    def __init__(self, nb, dtype, reps: Replicas, kernel=KERNEL_AUTO, stream=None, arith=None, overlap=True,
+                 stepper=None, state=None):
+        import torch
+
         self.torch, self.reps = torch, reps
         self.nb = tuple(int(n) for n in nb)
         self.T = dtype
-        self.kernel, self.stream = kernel, stream
+        self.overlap = overlap
         self.lo, self.hi = slab_rows(self.nb[0], reps.world, reps.rank)
         self.nb_local = (self.hi - self.lo + 1,) + self.nb[1:]
+        self.nv = len(self.nb)
+        self.row = int(np.prod([n + 2 for n in self.nb[1:]]))  # cells per X row (plane)
         # constants of the whole domain (DX, C_min), not of the slab
         self.phys = Physics(dtype, self.nb)
-        self.phys_local = Physics(dtype, self.nb_local)
-        for f in ("D", "min_spacing", "Cc", "C_min"):
-            setattr(self.phys_local, f, getattr(self.phys, f))
-        self.cur = alloc_state(self.nb_local, dtype)
-        self.nxt = alloc_state(self.nb_local, dtype)
+        self.stream = stream
+        self.stepper = stepper or _gpu_stepper(stream, kernel, arith)
         tdt = torch.float64 if dtype is np.float64 else torch.float32
-        self.dt_dev = torch.zeros(1, dtype=tdt, device="cuda")
-        # the reference blast of the whole domain, seen from this slab's rows
-        g = Blast(nb=self.nb, rho_in=1.0, rho_out=1.2, p_in=10.0, p_out=0.1)
-        local = Blast(nb=self.nb_local, centre=(g.centre[0] - (self.lo - 1),) + tuple(g.centre[1:]), radius=g.radius,
-                      rho_in=1.0, rho_out=1.2, p_in=10.0, p_out=0.1)
-        first = init_blast_at(self.cur, self.phys_local, local, stream=stream)
-        first = self._min(first)
+        if state is None:
+            self.device = "cuda"
+            self.cur = alloc_state(self.nb_local, dtype)
+            self.nxt = alloc_state(self.nb_local, dtype)
+            # the reference blast of the whole domain, seen from this slab's rows
+            g = Blast(nb=self.nb, rho_in=1.0, rho_out=1.2, p_in=10.0, p_out=0.1)
+            local = Blast(nb=self.nb_local, centre=(g.centre[0] - (self.lo - 1),) + tuple(g.centre[1:]),
+                          radius=g.radius, rho_in=1.0, rho_out=1.2, p_in=10.0, p_out=0.1)
+            first = init_blast_at(self.cur, self._phys_rows(self.nb_local[0]), local, stream=stream)
+        else:
+            (self.cur, first) = state
+            self.device = self.cur[0].device.type
+            self.nxt = tuple(torch.zeros_like(a) for a in self.cur)
+        # one Dt scalar per updated part (edges, interior) and their minimum
+        self.dt_parts = torch.zeros(3, dtype=tdt, device=self.device)
+        self.dt_min = torch.zeros(1, dtype=tdt, device=self.device)
+        first = self._min_host(first)
         big = dtype(1e20)
         self.dt = first if first < big else big
         self.t, self.it = 0.0, 0
-        self.row = int(np.prod([n + 2 for n in self.nb[1:]]))  # cells per X row (plane)
+        self.infos = []
+        self._exchange_blocking(self.cur)
 
-    # -- collectives ----------------------------------------------------------------
-    def _min(self, x):
+    # -- views and parts ----------------------------------------------------------------
+    def _phys_rows(self, nrows):
+        p = Physics(self.T, (nrows,) + self.nb[1:])
+        for f in ("D", "min_spacing", "Cc", "C_min"):
+            setattr(p, f, getattr(self.phys, f))
+        return p
+
+    def _rows(self, a, i, j=None):
+        """View of X rows i .. j-1 (default: row i) of one state array."""
+        nv = a.numel() // ((self.nb_local[0] + 2) * self.row)
+        j = i + 1 if j is None else j
+        return a[i * self.row * nv:j * self.row * nv]
+
+    def _part(self, state, first, nrows):
+        """The state seen from row `first`: a view of rows first .. first+nrows+1, where the
+        step updates rows first+1 .. first+nrows from their neighbours."""
+        return tuple(self._rows(a, first, first + nrows + 2) for a in state)
+
+    def _update(self, first, nrows, k, sync):
+        phys = self._phys_rows(nrows)
+        info = self.stepper(self._part(self.cur, first, nrows), self._part(self.nxt, first, nrows),
+                            self.dt_parts[k:k + 1], phys, self.phys.dtd(self.dt), sync)
+        return info
+
+    # -- collectives ----------------------------------------------------------------------
+    def _min_host(self, x):
         if self.reps.world == 1:
             return x
         torch = self.torch
-        dev = "cuda" if self.reps.backend == "nccl" else "cpu"
-        t = torch.tensor([float(x)], dtype=torch.float64 if self.T is np.float64 else torch.float32, device=dev)
+        t = torch.tensor([float(x)], dtype=torch.float64 if self.T is np.float64 else torch.float32,
+                         device=self.reps.device)
         self.reps.dist.all_reduce(t, op=self.reps.dist.ReduceOp.MIN)
         return self.T(t.item())
 
-    def _rows(self, a, i):
-        """View of X row (plane) i of one state array (both components of the cell)."""
-        nv = a.numel() // ((self.nb_local[0] + 2) * self.row)
-        return a[i * self.row * nv:(i + 1) * self.row * nv]
-
-    def exchange(self):
-        """Fill the ghost rows 0 and NB_X_local+1 of the current state from the
-        neighbouring ranks' edge rows (periodic across ranks)."""
+    def _start_exchange(self, state):
+        """Start sending `state`'s edge rows to the neighbours and receiving theirs into
+        the ghost rows; returns the pending works and the copies that finish it."""
         n = self.nb_local[0]
         if self.reps.world == 1:
-            for a in self.cur:
+            for a in state:
                 self._rows(a, 0).copy_(self._rows(a, n))
                 self._rows(a, n + 1).copy_(self._rows(a, 1))
-            return
+            return [], []
         dist, torch = self.reps.dist, self.torch
         left = (self.reps.rank - 1) % self.reps.world
         right = (self.reps.rank + 1) % self.reps.world
-        staged = self.reps.backend != "nccl"
-        for a in self.cur:
+        staged = self.reps.backend != "nccl" and state[0].device.type == "cuda"
+        ops, finish = [], []
+        for a in state:
             first, last = self._rows(a, 1), self._rows(a, n)
             send_l = first.cpu() if staged else first.contiguous()
             send_r = last.cpu() if staged else last.contiguous()
@@ -101,20 +159,59 @@ class XSlabRun:
             # the rightward message (last row -> right neighbour's ghost row 0) first, then the
             # leftward one: with two ranks both neighbours are the same peer and messages
             # between a pair of ranks match in issue order (NCCL has no tags)
-            ops = [dist.P2POp(dist.isend, send_r, right, tag=1), dist.P2POp(dist.isend, send_l, left, tag=2),
-                   dist.P2POp(dist.irecv, recv_lo, left, tag=1), dist.P2POp(dist.irecv, recv_hi, right, tag=2)]
-            for r in dist.batch_isend_irecv(ops):
-                r.wait()
-            self._rows(a, 0).copy_(recv_lo)       # left neighbour's last row
-            self._rows(a, n + 1).copy_(recv_hi)   # right neighbour's first row
+            ops += [dist.P2POp(dist.isend, send_r, right, tag=1), dist.P2POp(dist.isend, send_l, left, tag=2),
+                    dist.P2POp(dist.irecv, recv_lo, left, tag=1), dist.P2POp(dist.irecv, recv_hi, right, tag=2)]
+            finish.append((self._rows(a, 0), recv_lo))       # left neighbour's last row
+            finish.append((self._rows(a, n + 1), recv_hi))   # right neighbour's first row
+        return dist.batch_isend_irecv(ops), finish
 
+    @staticmethod
+    def _finish_exchange(works, finish):
+        for w in works:
+            w.wait()
+        for dst, src in finish:
+            dst.copy_(src)
+
+    def _exchange_blocking(self, state):
+        self._finish_exchange(*self._start_exchange(state))
+
+    def exchange(self):
+        """Fill the ghost rows 0 and NB_X_local+1 of the current state from the
+        neighbouring ranks' edge rows (periodic across ranks)."""
+        self._exchange_blocking(self.cur)
+
+    # -- the step -------------------------------------------------------------------------
     def step(self):
-        self.exchange()
-        dtd = self.phys.dtd(self.dt)
-        step(self.cur, self.nxt, self.dt_dev, self.phys_local, dtd, kernel=self.kernel, sync=True,
-             stream=self.stream, x_ghosts=True)
+        n = self.nb_local[0]
+        self.dt_parts.fill_(float("inf"))
+        self.infos = []
+        if not self.overlap or n <= 2:
+            # the whole slab in one update, then the exchange for the next step
+            self.infos.append(self._update(0, n, 0, True))
+            self._exchange_blocking(self.nxt)
+        else:
+            # edge rows first, their exchange in flight while the interior is updated
+            self.infos.append(self._update(0, 1, 0, True))
+            self.infos.append(self._update(n - 1, 1, 1, True))
+            pending = self._start_exchange(self.nxt)
+            self.infos.append(self._update(1, n - 2, 2, False))
+            self._finish_exchange(*pending)
+        torch = self.torch
+        torch.amin(self.dt_parts, dim=0, keepdim=True, out=self.dt_min)
+        if self.reps.world > 1:
+            dt = self.dt_min
+            if self.reps.backend != "nccl" and dt.device.type == "cuda":
+                dt = dt.cpu()
+            self.reps.dist.all_reduce(dt, op=self.reps.dist.ReduceOp.MIN)
+            dtn = self.T(dt.item())
+        else:
+            dtn = self.T(self.dt_min.item())
+        if self.overlap and n > 2 and self.device == "cuda":
+            # the interior update was enqueued without waiting: its status, now complete
+            info = StepInfo()
+            _check(lib().hydro_last_step_info(ctypes.byref(info)))
+            self.infos[-1] = info
         self.cur, self.nxt = self.nxt, self.cur
-        dtn = self._min(self.T(self.dt_dev.item()))
         big = self.T(1e20)
         self.dt = dtn if dtn < big else big
         self.it += 1

@@ -76,3 +76,21 @@ def test_noalloc_launch_shape_fits_the_fixed_scratch(built):
     fn(100000, 126 * 4096, 1, 148, ctypes.byref(c), ctypes.byref(gx), ctypes.byref(gy))
     assert (c.value, gy.value) == (6250, 16)
     assert fn(10, 126 * 65536 + 1, 1, 148, ctypes.byref(c), ctypes.byref(gx), ctypes.byref(gy)) == 0
+
+
+def test_launch_shape_settings(built):
+    """hydro_set_launch_shape (host only): the tile heights the 3D kernels are built for are
+    accepted, others and 2D tile heights rejected with HYDRO_ERR_ARG; 0 restores the
+    built-in shape."""
+    fn = built.hydro_set_launch_shape
+    fn.argtypes = [ctypes.c_int] * 4
+    fn.restype = ctypes.c_int
+    for dim, pb, w, c in ((3, 8, 8, 0), (3, 8, 12, 64), (3, 8, 16, 32), (3, 4, 8, 0), (3, 4, 16, 128),
+                          (2, 8, 0, 64), (2, 4, 0, 0)):
+        assert fn(dim, pb, w, c) == 0, (dim, pb, w, c)
+    for dim, pb, w, c in ((3, 4, 12, 0), (3, 8, 10, 0), (2, 8, 8, 0), (4, 8, 0, 0), (3, 2, 8, 0), (3, 8, 8, -1)):
+        assert fn(dim, pb, w, c) == hb.HYDRO_ERR_ARG, (dim, pb, w, c)
+    for dim in (2, 3):
+        for pb in (4, 8):
+            assert fn(dim, pb, 0, 0) == 0
+    built.hydro_clear_error()

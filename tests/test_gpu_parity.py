@@ -33,7 +33,7 @@ def gpu_step(cuda, st_host, phys, dtd, kernel):
     nxt = tuple(cuda.zeros_like(a) for a in cur)
     tdt = cur[0].dtype
     dt = cuda.zeros(1, dtype=tdt, device="cuda")
-    _, info = hb.step(cur, nxt, dt, phys, dtd, kernel=kernel)
+    _, info = hb.step(cur, nxt, dt, phys, dtd, kernel=kernel, arith="strict")
     return tuple(a.cpu().numpy() for a in nxt), phys.dtype(dt.item()), info
 
 
@@ -299,3 +299,33 @@ def test_step_x_ghosts_from_memory(cuda, oracle, nb, T, kernel):
         assert phys.dtype(dt.item()).tobytes() == dref.tobytes()
         out = tuple(a.cpu().numpy() for a in nxt)
         assert out[0].tobytes() == ref[0].tobytes() and out[1].tobytes() == ref[1].tobytes()
+
+
+@pytest.mark.parametrize("T", [np.float64, np.float32])
+def test_launch_shapes_bitwise(cuda, oracle, T):
+    """Every tile height and chunk the autotuner may pick gives the oracle's bits: 3D tile
+    heights (8, 12, 16 warps in FP64; 8, 16 in FP32) and explicit chunks, 2D chunks."""
+    warps = (8, 12, 16) if T is np.float64 else (8, 16)
+    cases = [((40, 150, 130), w, c) for w in warps for c in (0, 7, 64)] + \
+            [((9, 14, 62), w, 3) for w in warps] + [((300, 253), 0, c) for c in (0, 5, 300)]
+    try:
+        for nb, w, c in cases:
+            phys = hb.Physics(T, nb)
+            hb.set_launch_shape(len(nb), T, w, c)
+            st = seeded_state(nb, T, 4)
+            oracle.ghost_x(st, nb)
+            ref = (np.zeros_like(st[0]), np.zeros_like(st[1]))
+            dtd = phys.dtd(cfl_dt(phys, 4))
+            dref = oracle.step(st, ref, phys, dtd)
+            out, d, info = gpu_step(cuda, st, phys, dtd, hb.KERNEL_STRIP)
+            shape = hb.last_launch_shape()
+            if len(nb) == 3:
+                assert shape["warps"] == w
+            if c:
+                assert shape["chunk"] == c
+            assert d.tobytes() == dref.tobytes(), (nb, w, c)
+            assert out[0].tobytes() == ref[0].tobytes(), (nb, w, c)
+            assert out[1].tobytes() == ref[1].tobytes(), (nb, w, c)
+    finally:
+        for dim in (2, 3):
+            hb.set_launch_shape(dim, T, 0, 0)

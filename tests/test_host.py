@@ -180,7 +180,7 @@ def _slab_rank_main(rank, world, port, nb, q):
         run.exchange()
         ghosts = [(a.numpy().reshape(n + 2, run.row, -1)[0].copy(), a.numpy().reshape(n + 2, run.row, -1)[n + 1].copy())
                   for a in run.cur]
-        dt = run._min(0.25 + rank)
+        dt = run._min_host(0.25 + rank)
         reps.barrier()
         reps.close()
         q.put((rank, run.lo, run.hi, ghosts, float(dt)))
@@ -301,3 +301,88 @@ def test_server_admission_on_cpu():
     assert admitted == sorted(admitted)
     # continuous batching: the second request joined while the first was still running
     assert recs[1].admit < recs[0].done
+
+
+def _oracle_slab_rank(rank, world, port, nb, steps, overlap, q):
+    """One gloo rank stepping its slab with the oracle on the host through XSlabRun's
+    schedule (edge rows, their exchange, interior rows, Dt MIN); reports its interior,
+    t and Dt."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    try:
+        import torch
+
+        from conftest import load_pkg as _load
+
+        _load()
+        import oracle as orc
+        from hydro_b200 import Physics
+        from hydro_b200.replicas import Replicas
+        from hydro_b200.slabs import XSlabRun, slab_rows
+
+        o = orc.Oracle()
+        T = np.float64
+        phys = Physics(T, nb)
+        full = tuple(np.zeros(int(np.prod([n + 2 for n in nb])) * k, T) for k in (2, len(nb)))
+        first = o.init(full, phys)
+        lo, hi = slab_rows(nb[0], world, rank)
+        row = int(np.prod([n + 2 for n in nb[1:]]))
+        state = tuple(torch.from_numpy(a[(lo - 1) * row * k:(hi + 2) * row * k].copy())
+                      for a, k in zip(full, (2, len(nb))))
+
+        def stepper(cur, nxt, dt_out, p, dtd, sync):
+            d = o.step(tuple(a.numpy() for a in cur), tuple(a.numpy() for a in nxt), p, dtd)
+            dt_out.fill_(float(d))
+            return None
+
+        reps = Replicas("gloo", timeout_s=60)
+        run = XSlabRun(nb, T, reps, overlap=overlap, stepper=stepper, state=(state, first)).run(1e9, steps)
+        out = run.interior()
+        reps.barrier()
+        reps.close()
+        q.put((rank, lo, hi, [a.copy() for a in out], run.t, float(run.dt)))
+    except Exception as e:  # reported to the parent
+        import traceback
+
+        q.put((rank, traceback.format_exc(), None, None, None, None))
+
+
+@pytest.mark.parametrize("overlap", [True, False])
+@pytest.mark.parametrize("world,nb", [(2, (13, 9)), (3, (11, 6)), (2, (9, 6, 5)), (3, (8, 5, 4))])
+def test_slab_schedule_gloo_matches_whole_domain(world, nb, overlap):
+    """XSlabRun's step schedule across gloo ranks on CPU, with the oracle as the step: the
+    edge rows first, their exchange in flight while the interior rows are updated, then
+    the Dt MIN over ranks (overlap), or the whole slab then the exchange. After six steps
+    the gathered slabs are bit-identical to the whole domain stepped by the oracle with
+    periodic X ghosts, with the same t and Dt."""
+    import multiprocessing as mp
+
+    import oracle as orc
+    from hydro_b200 import Physics
+
+    steps = 6
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_oracle_slab_rank, args=(r, world, port, nb, steps, overlap, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted((q.get(timeout=180) for _ in procs), key=lambda o: o[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, lo, *_ in out:
+        assert out[rank][3] is not None, lo
+    o = orc.Oracle()
+    T = np.float64
+    phys = Physics(T, nb)
+    full = tuple(np.zeros(int(np.prod([n + 2 for n in nb])) * k, T) for k in (2, len(nb)))
+    first = o.init(full, phys)
+    ref, t_log, dt_log = orc.host_loop(o.step, full, phys, first, 1e9, steps)
+    want = orc.interior(ref, nb)
+    for k in range(2):
+        got = np.concatenate([r[3][k] for r in out], axis=0)
+        assert got.tobytes() == np.ascontiguousarray(want[k]).tobytes()
+    for rank, lo, hi, _, t, dt in out:
+        assert t == t_log[-1] + float(dt_log[-1]) and dt == float(dt_log[-1])
