@@ -305,6 +305,10 @@ int hydro_batch_prepare(void *batch, int nsteps);
  * a step where no cell does takes an exact pass over all the instance's cells. Dt is the
  * exact value whatever `frac` is (default 0.9; 0 computes every cell exactly). */
 int hydro_batch_set_skip_fraction(void *batch, double frac);
+/* Arithmetic of the batch's step kernels: HYDRO_ARITH_STRICT (default) or
+ * HYDRO_ARITH_FUSED, as for the plain steps; an instance's state stays bit-identical to the
+ * plain path in the same precision and arithmetic. Takes effect at the next run. */
+int hydro_batch_set_arith(void *batch, int arith);
 void hydro_batch_destroy(void *batch);
 
 /* The blast initial condition of hydro2d/main.cxx:280-338 (hydro3d/main.cxx:296-363) with

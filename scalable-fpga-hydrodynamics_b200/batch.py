@@ -96,6 +96,8 @@ def _declare(L):
     L.hydro_batch_prepare.restype = _c.c_int
     L.hydro_batch_set_skip_fraction.argtypes = [vp, _c.c_double]
     L.hydro_batch_set_skip_fraction.restype = _c.c_int
+    L.hydro_batch_set_arith.argtypes = [vp, _c.c_int]
+    L.hydro_batch_set_arith.restype = _c.c_int
     L._batch_declared = True
     return L
 
@@ -103,7 +105,9 @@ def _declare(L):
 class Batch:
     """A set of blast instances advanced together (2D; FP32 or FP64)."""
 
-    def __init__(self, dim: int = 2, dtype=np.float32, chunk: int = 0, capacity: int = 1024, stream=None):
+    def __init__(self, dim: int = 2, dtype=np.float32, chunk: int = 0, capacity: int = 1024, stream=None,
+                 arith=None):
+        """arith: "strict", "fused" or None (the library default)."""
         torch = _torch()
         self.L = _declare(lib())
         self.dim, self.T = dim, dtype
@@ -113,6 +117,10 @@ class Batch:
         if not self.h:
             raise HydroError(*last_error())
         self.blasts = {}
+        if arith is not None:
+            from . import _ARITH_BITS
+
+            _check(self.L.hydro_batch_set_arith(self.h, _ARITH_BITS[arith]))
 
     def close(self):
         if self.h:

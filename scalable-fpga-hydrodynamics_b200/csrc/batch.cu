@@ -192,7 +192,7 @@ template <int NT> __device__ __forceinline__ double block_max(double v, unsigned
     if (__syncthreads_or(err != 0)) err = kErrNonPhysical;
     return __longlong_as_double((long long)mb);
 }
-template <int NT, class T> __device__ double exact_max(const Inst2<T> *in, unsigned &err)
+template <int NT, class T, bool kF> __device__ double exact_max(const Inst2<T> *in, unsigned &err)
 {
     const int b = in->parity ^ 1;
     const T *r = in->rhoE[b], *u = in->uv[b];
@@ -200,14 +200,14 @@ template <int NT, class T> __device__ double exact_max(const Inst2<T> *in, unsig
     double vmax = 0.0;
     for (long long q = threadIdx.x; q < n; q += NT) {
         const long long c = (1 + q / ny) * in->ys + 1 + q % ny;
-        const double sp = (double)speed2(__ldcg(r + 2 * c), __ldcg(u + 2 * c), __ldcg(u + 2 * c + 1),
-                                         __ldcg(r + 2 * c + 1), in->ph);
+        const double sp = (double)speed2<T, kF>(__ldcg(r + 2 * c), __ldcg(u + 2 * c), __ldcg(u + 2 * c + 1),
+                                                __ldcg(r + 2 * c + 1), in->ph);
         vmax = (sp > vmax) ? sp : vmax;
         if (!(sp <= 1.0e300)) err = kErrNonPhysical;
     }
     return block_max<NT>(vmax, err);
 }
-template <int NT, class T> __device__ double exact_max(const Inst3<T> *in, unsigned &err)
+template <int NT, class T, bool kF> __device__ double exact_max(const Inst3<T> *in, unsigned &err)
 {
     const int b = in->parity ^ 1;
     const T *r = in->rhoE[b], *u = in->uvw[b];
@@ -216,8 +216,8 @@ template <int NT, class T> __device__ double exact_max(const Inst3<T> *in, unsig
     for (long long q = threadIdx.x; q < n; q += NT) {
         const long long rr = q % ncol;
         const long long c = (1 + q / ncol) * in->zy + (1 + rr / in->nb_z) * in->zs + 1 + rr % in->nb_z;
-        const double sp = (double)speed3(__ldcg(r + 2 * c), __ldcg(u + 3 * c), __ldcg(u + 3 * c + 1),
-                                         __ldcg(u + 3 * c + 2), __ldcg(r + 2 * c + 1), in->ph);
+        const double sp = (double)speed3<T, kF>(__ldcg(r + 2 * c), __ldcg(u + 3 * c), __ldcg(u + 3 * c + 1),
+                                                __ldcg(u + 3 * c + 2), __ldcg(r + 2 * c + 1), in->ph);
         vmax = (sp > vmax) ? sp : vmax;
         if (!(sp <= 1.0e300)) err = kErrNonPhysical;
     }
@@ -273,7 +273,7 @@ template <int NT> __device__ __forceinline__ double block_max_err(double v, unsi
 
 // Merge an instance's item maxima, take the exact pass if no cell reached the skip
 // threshold, and advance the instance (whole block).
-template <int NT, class T, class I>
+template <int NT, class T, bool kF, class I>
 __device__ void finalize_step(I *in, const ItemPart *parts, int nitems, SlotStatus *st, double skip_frac)
 {
     unsigned long long mb = 0ull;
@@ -291,7 +291,7 @@ __device__ void finalize_step(I *in, const ItemPart *parts, int nitems, SlotStat
     __syncthreads();
     if (s_redo) {
         unsigned e2 = 0;
-        const double m = exact_max<NT, T>(in, e2);
+        const double m = exact_max<NT, T, kF>(in, e2);
         if (threadIdx.x == 0) {
             vmax = m;
             err |= e2;
@@ -369,7 +369,8 @@ __device__ __forceinline__ bool publish_item(BatchAcc &acc, ItemPart *parts, int
 // resident blocks per SM the register budget of the 2D step aims at
 template <class T> struct Batch2dOcc { static constexpr int value = sizeof(T) == 4 ? 6 : 4; };
 
-template <class T>
+// kF: fused arithmetic (hydro_math.cuh)
+template <class T, bool kF>
 __global__ void __launch_bounds__(kStripNT, Batch2dOcc<T>::value) batch2d(Inst2<T> *insts, const int2 *items, const int2 *ranges,
                                                       int nitems, unsigned *counter, ItemPart *parts,
                                                       SlotStatus *status, double skip_frac)
@@ -399,21 +400,21 @@ __global__ void __launch_bounds__(kStripNT, Batch2dOcc<T>::value) batch2d(Inst2<
         }
         MaxAcc acc;
         const float tlo2 = skip_tlo2(batch_threshold(I, skip_frac)), ggm1 = I->ggm1;
-        const bool ok = march2d<T>(S, &I->tm[par][0], &I->tm[par][1], geo, I->rhoE[par ^ 1], I->uv[par ^ 1], ph,
+        const bool ok = march2d<T, true, kF>(S, &I->tm[par][0], &I->tm[par][1], geo, I->rhoE[par ^ 1], I->uv[par ^ 1], ph,
                                    I->DtDx, I->DtDy, ld, [&](const Upd2<T> &o) {
                                        if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
                                        const float fu = (float)o.u, fv = (float)o.v;
                                        if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1, tlo2))
-                                           acc.add_speed((double)speed2(o.r, o.u, o.v, o.E, ph));
+                                           acc.add_speed((double)speed2<T, kF>(o.r, o.u, o.v, o.E, ph));
                                    });
         if (!ok) acc.err |= kErrWaitTimeout;
         const int2 rg = ranges[it.x];
         if (publish_step<kStripNT>(acc, parts, w, &I->done_items, rg.y, &s_last))
-            finalize_step<kStripNT, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
+            finalize_step<kStripNT, T, kF>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
     }
 }
 
-template <class T>
+template <class T, bool kF>
 __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) batch3d(Inst3<T> *insts, const int2 *items, const int2 *ranges,
                                                   int nitems, unsigned *counter, ItemPart *parts,
                                                   SlotStatus *status, double skip_frac)
@@ -440,16 +441,16 @@ __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) batch3d(Inst3<T> *ins
         const Phys<T> ph = I->ph;
         MaxAcc acc;
         const float tlo2 = skip_tlo2(batch_threshold(I, skip_frac)), ggm1 = I->ggm1;
-        march3d<T>(S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy,
+        march3d<T, kF>(S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy,
                    I->DtDz, [&](const Upd3<T> &o) {
                        if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
                        const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
                        if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1, tlo2))
-                           acc.add_speed((double)speed3(o.r, o.u, o.v, o.w, o.E, ph));
+                           acc.add_speed((double)speed3<T, kF>(o.r, o.u, o.v, o.w, o.E, ph));
                    });
         const int2 rg = ranges[it.x];
         if (publish_step<k3NT<T>>(acc, parts, w, &I->done_items, rg.y, &s_last))
-            finalize_step<k3NT<T>, T>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
+            finalize_step<k3NT<T>, T, kF>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);
     }
 }
 
@@ -521,6 +522,7 @@ class BatchBase {
     virtual int sync() = 0;
     virtual int prepare(int nsteps) = 0;
     virtual int set_skip_fraction(double f) = 0;
+    virtual int set_arith(bool fused) = 0;
 };
 
 template <class T, int D> class BatchEngine final : public BatchBase {
@@ -545,15 +547,24 @@ template <class T, int D> class BatchEngine final : public BatchBase {
         int dev = 0, nsm = 1, occ = 1;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        // persistent grid: the resident blocks of the step kernel (the smaller of the
+        // strict and fused variants' occupancy)
+        int occ_f = 1;
         if constexpr (D == 2) {
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch2d<T>, kStripNT, 0);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch2d<T, false>, kStripNT, 0);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, batch2d<T, true>, kStripNT, 0);
         } else {
             smem_ = (int)sizeof(Smem3<T>);
             if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(batch3d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_);
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch3d<T>, k3NT<T>, smem_);
+                e = cudaFuncSetAttribute(batch3d<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(batch3d<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch3d<T, false>, k3NT<T>, smem_);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, batch3d<T, true>, k3NT<T>, smem_);
         }
-        blocks_ = nsm * std::max(1, occ);
+        blocks_ = nsm * std::max(1, std::min(occ, occ_f));
         int occ_s = 0;
         if (e == cudaSuccess) {
             if constexpr (D == 2)
@@ -836,6 +847,13 @@ template <class T, int D> class BatchEngine final : public BatchBase {
         return kOk;
     }
 
+    int set_arith(bool fused) override
+    {
+        fused_ = fused;
+        dirty_ = true; // the step kernel of the captured graph changes
+        return kOk;
+    }
+
     int prepare(int nsteps) override
     {
         if (nsteps < 0) {
@@ -876,12 +894,15 @@ template <class T, int D> class BatchEngine final : public BatchBase {
 
     void launch()
     {
-        if constexpr (D == 2)
-            batch2d<T><<<blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
-                                                         status_d_, skip_frac_);
-        else
-            batch3d<T><<<blocks_, k3NT<T>, smem_, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_,
-                                                         status_d_, skip_frac_);
+        if constexpr (D == 2) {
+            auto k = fused_ ? batch2d<T, true> : batch2d<T, false>;
+            k<<<blocks_, kStripNT, 0, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_, status_d_,
+                                                 skip_frac_);
+        } else {
+            auto k = fused_ ? batch3d<T, true> : batch3d<T, false>;
+            k<<<blocks_, k3NT<T>, smem_, stream_>>>(insts_, items_, ranges_, nitems_, counter_, parts_, status_d_,
+                                                   skip_frac_);
+        }
     }
 
     void launch_sums()
@@ -960,6 +981,7 @@ template <class T, int D> class BatchEngine final : public BatchBase {
 
     int chunk_, cap_;
     double skip_frac_ = kSkipFrac;
+    bool fused_ = false; // fused arithmetic of the step kernels (hydro_batch_set_arith)
     bool own_stream_ = false, dirty_ = true;
     cudaStream_t stream_ = nullptr;
     Inst *insts_ = nullptr;
@@ -1052,6 +1074,15 @@ int hydro_batch_prepare(void *b, int nsteps)
 {
     if (!b) return kErrArg;
     return static_cast<BatchBase *>(b)->prepare(nsteps);
+}
+
+int hydro_batch_set_arith(void *b, int arith)
+{
+    if (!b || (arith & ~(HYDRO_ARITH_FUSED | HYDRO_ARITH_STRICT))) {
+        set_error(kErrArg, "hydro_batch_set_arith: null batch or unknown bits 0x%x", arith);
+        return kErrArg;
+    }
+    return static_cast<BatchBase *>(b)->set_arith((arith & HYDRO_ARITH_FUSED) && !(arith & HYDRO_ARITH_STRICT));
 }
 
 int hydro_batch_set_skip_fraction(void *b, double frac)

@@ -17,16 +17,17 @@ def interior(st, nb):
     return orc.interior(st, nb)
 
 
+@pytest.mark.parametrize("arith", ["strict", "fused"])
 @pytest.mark.parametrize("T", [np.float64, np.float32])
-def test_batch_instance_equals_plain_path(cuda, T):
+def test_batch_instance_equals_plain_path(cuda, T, arith):
     """The reference blast through the batch (with other instances around it) and through
-    the plain path: same Dt sequence end, same t, same interior bits."""
+    the plain path in the same arithmetic: same Dt sequence end, same t, same interior bits."""
     from hydro_b200.batch import Batch, Blast
 
     nb = (300, 250) if T is np.float64 else (300, 252)
     steps = 40
-    plain = hb.BlastRun(nb, T).run(1e9, steps)
-    b = Batch(2, T, capacity=8)
+    plain = hb.BlastRun(nb, T, arith=arith).run(1e9, steps)
+    b = Batch(2, T, capacity=8, arith=arith)
     others = [b.add(Blast(nb=(97, 131), max_steps=steps + 5)), b.add(Blast(nb=(64, 500), max_steps=3))]
     slot = b.add(Blast(nb=nb, max_steps=steps))
     b.run(steps + 5)
@@ -111,17 +112,19 @@ def test_batch_retire_remove_reuse(cuda):
     b.close()
 
 
+@pytest.mark.parametrize("arith", ["strict", "fused"])
 @pytest.mark.parametrize("T", [np.float64, np.float32])
-def test_batch3d_instance_equals_plain_path(cuda, T):
+def test_batch3d_instance_equals_plain_path(cuda, T, arith):
     """A 3D blast through the 3D batch (beside two other instances) and through the plain
-    3D path: same t, same Dt, same interior bits."""
+    3D path in the same arithmetic: same t, same Dt, same interior bits (the plain FP64
+    path stages its planes by tensor maps here, the batch by per-lane copies)."""
     from hydro_b200.batch import Batch, Blast
 
     nb = (40, 36, 30)
     steps = 25
     bl = Blast(nb=nb, max_steps=steps)
-    plain = hb.BlastRun(nb, T, blast=bl).run(1e9, steps)
-    b = Batch(3, T, capacity=4)
+    plain = hb.BlastRun(nb, T, blast=bl, arith=arith).run(1e9, steps)
+    b = Batch(3, T, capacity=4, arith=arith)
     b.add(Blast(nb=(20, 50, 17), max_steps=steps + 3))
     b.add(Blast(nb=(33, 12, 40), max_steps=4))
     slot = b.add(bl)
