@@ -830,7 +830,7 @@ def main():
         key = f"{len(vnb)}d_{np.dtype(T).name}_{ar}"
         if key not in tuned:
             tuned[key] = tune_plain(vnb, T, ar, log=log)
-        hb.set_launch_shape(len(vnb), T, tuned[key]["warps"], tuned[key]["chunk"])
+        hb.set_launch_shape(len(vnb), T, tuned[key]["warps"], tuned[key]["chunk"], tuned[key].get("blocks", 0))
         return tuned[key]
 
     tune(nb, Tcase, args.arith)
@@ -944,7 +944,8 @@ def main():
         if accuracy:
             line["accuracy_vs_strict_fp64"] = accuracy
         if tuned:
-            line["autotuned_shapes"] = {k: dict(warps=v["warps"], chunk=v["chunk"]) for k, v in tuned.items()}
+            line["autotuned_shapes"] = {k: dict(warps=v["warps"], blocks=v.get("blocks", 0), chunk=v["chunk"])
+                                        for k, v in tuned.items()}
         line["energy"] = energy_entry(r["energy_j"], total_ms / 1e3, cells * args.steps)
         line["variants"] = variants
         line["batched"] = batched

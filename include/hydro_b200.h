@@ -195,16 +195,19 @@ unsigned hydro2d_noalloc_launch_shape(size_t NB_X, size_t NB_Y, int strip, int s
                                       unsigned *grid_y);
 
 /* Launch shape of the plain strip kernels for (dim 2 or 3, precision 4 or 8 bytes), as an
- * autotuner picks it: `warps` = warps per block of the 3D kernel, i.e. tile rows with the
- * halo (8, 16, and 12 in FP64; 0 = built-in: 8 in FP64, 16 in FP32; must be 0 in 2D), and
- * `chunk` = rows (2D) or planes (3D) each block marches (0 = sized from the grid and the
- * SM count). Process-wide; the results do not depend on the shape. No counterpart in the
- * reference, whose single-task kernel has no launch shape. */
-int hydro_set_launch_shape(int dim, int precision_bytes, int warps, int chunk);
-/* The shape the last strip-kernel step on the current device used: warps per block (0 in
- * 2D), rows or planes per block, and whether its rows / planes were staged by tensor-map
- * loads (1) or per-lane copies (0). */
-int hydro_last_launch_shape(int *warps, int *chunk, int *tma);
+ * autotuner picks it. 0 keeps the built-in choice for any field.
+ *  warps: 3D only, warps per block, i.e. tile rows with the one-row halo (8, 16, and 12 in
+ *    FP64; built-in 8 in FP64, 16 in FP32);
+ *  chunk: rows (2D) or planes (3D) each block marches (built-in: sized from the grid and
+ *    the SM count);
+ *  blocks_per_sm: 2D only, the resident blocks per SM the kernel's registers are budgeted
+ *    for (4, or 5 in FP64 / 8 in FP32; built-in 4).
+ * Process-wide; the results do not depend on the shape. No counterpart in the reference,
+ * whose single-task kernel has no launch shape. */
+int hydro_set_launch_shape(int dim, int precision_bytes, int warps, int chunk, int blocks_per_sm);
+/* The shape the last strip-kernel step on the current device used (warps 0 in 2D), and
+ * whether its rows / planes were staged by tensor-map loads (1) or per-lane copies (0). */
+int hydro_last_launch_shape(int *warps, int *chunk, int *blocks_per_sm, int *tma);
 
 /* Diagnostics: the number of per-device contexts (scratch words, partial sums, a pinned
  * status record) the regular entry points have created in this process. The

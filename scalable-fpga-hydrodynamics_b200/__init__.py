@@ -99,9 +99,9 @@ def _declare(lib):
         fn = getattr(lib, f"hydro_mass_{suf}")
         fn.argtypes = [_vp, _c_size, _c_size, _c_size, pd, _vp]
         fn.restype = ctypes.c_int
-    lib.hydro_set_launch_shape.argtypes = [ctypes.c_int] * 4
+    lib.hydro_set_launch_shape.argtypes = [ctypes.c_int] * 5
     lib.hydro_set_launch_shape.restype = ctypes.c_int
-    lib.hydro_last_launch_shape.argtypes = [ctypes.POINTER(ctypes.c_int)] * 3
+    lib.hydro_last_launch_shape.argtypes = [ctypes.POINTER(ctypes.c_int)] * 4
     lib.hydro_last_launch_shape.restype = ctypes.c_int
     lib.hydro_last_step_info.argtypes = [ctypes.POINTER(StepInfo)]
     lib.hydro_last_step_info.restype = ctypes.c_int
@@ -122,18 +122,18 @@ def lib():
     return _lib
 
 
-def set_launch_shape(dim: int, dtype, warps: int = 0, chunk: int = 0):
+def set_launch_shape(dim: int, dtype, warps: int = 0, chunk: int = 0, blocks: int = 0):
     """Launch shape of the plain strip kernels for (dim, precision): 3D warps per block
-    (tile rows with halo; 0 = built-in) and rows / planes per block (0 = sized from the
-    grid). Results do not depend on it."""
-    _check(lib().hydro_set_launch_shape(int(dim), np.dtype(dtype).itemsize, int(warps), int(chunk)))
+    (tile rows with halo), rows / planes per block, 2D register budget in blocks per SM
+    (0 = built-in for each). Results do not depend on it."""
+    _check(lib().hydro_set_launch_shape(int(dim), np.dtype(dtype).itemsize, int(warps), int(chunk), int(blocks)))
 
 
 def last_launch_shape() -> dict:
     """The shape the last strip-kernel step on the current device used."""
-    w, c, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-    _check(lib().hydro_last_launch_shape(ctypes.byref(w), ctypes.byref(c), ctypes.byref(t)))
-    return dict(warps=w.value, chunk=c.value, tma=bool(t.value))
+    w, c, b, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().hydro_last_launch_shape(ctypes.byref(w), ctypes.byref(c), ctypes.byref(b), ctypes.byref(t)))
+    return dict(warps=w.value, chunk=c.value, blocks=b.value, tma=bool(t.value))
 
 
 def last_error() -> tuple[int, str]:

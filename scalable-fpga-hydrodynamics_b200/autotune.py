@@ -1,13 +1,15 @@
 """Tile-shape autotuner, keyed on dimensionality and precision.
 
-Plain path (`tune_plain`): the strip kernels take two shape parameters, the tile height of
-the 3D kernel (warps per block, i.e. tile rows with the one-row halo: 8, 12 or 16 in FP64,
-8 or 16 in FP32) and the number of X rows (2D) or planes (3D) each block marches (`chunk`,
-or 0 for the built-in size from the grid and the SM count). Taller tiles recompute fewer
-halo rows but hold one block per SM; longer chunks re-read fewer halo rows but give fewer
-blocks. `tune_plain` times a few steps of the blast on the grid it is given for every
-candidate (warps x chunk), keeps the fastest and installs it in the library
-(hydro_set_launch_shape); the results do not depend on the shape.
+Plain path (`tune_plain`): the strip kernels take two shape parameters each. Both take the
+number of X rows (2D) or planes (3D) each block marches (`chunk`, or 0 for the built-in
+size from the grid and the SM count): longer chunks re-read fewer halo rows but give fewer
+blocks. The 3D kernel also takes its tile height (warps per block, i.e. tile rows with the
+one-row halo: 8, 12 or 16 in FP64, 8 or 16 in FP32): taller tiles recompute fewer halo
+rows but hold one block per SM. The 2D kernel also takes its register budget in resident
+blocks per SM (4, or 5 in FP64 / 8 in FP32): more resident warps against fewer registers
+per thread. `tune_plain` times a few steps of the blast on the grid it is given for every
+candidate, keeps the fastest and installs it in the library (hydro_set_launch_shape); the
+results do not depend on the shape.
 
 Batched path (`tune`): the batched kernels take a fixed block shape (2D: 128 lanes over
 126 interior columns; 3D: 8 x 32 lanes over 6 x 30 interior columns in FP64, 16 x 32 over
@@ -107,17 +109,19 @@ def best_chunk(dim, dtype):
     return int(entry["chunk"]) if entry else 0
 
 
-# plain-path candidates: 3D tile heights (warps per block) per precision, and chunks
-PLAIN_WARPS = {(2, 4): (0,), (2, 8): (0,), (3, 4): (8, 16), (3, 8): (8, 12, 16)}
+# plain-path candidates per (dim, precision bytes): (3D warps per block or 2D blocks per
+# SM, the other 0) and chunks
+PLAIN_SHAPES = {(2, 4): [(0, 4), (0, 8)], (2, 8): [(0, 4), (0, 5)], (3, 4): [(8, 0), (16, 0)],
+                (3, 8): [(8, 0), (12, 0), (16, 0)]}
 PLAIN_CHUNKS = {2: (0, 32, 64, 128, 256), 3: (0, 16, 32, 64, 128)}
 
 
-def measure_plain(nb, dtype, arith, warps, chunk, steps=4, warmup=2):
+def measure_plain(nb, dtype, arith, warps, chunk, blocks=0, steps=4, warmup=2):
     """Cell-updates per second of the plain path with one launch shape (CUDA events around
     `steps` steps after `warmup`), on the blast of grid `nb`."""
     torch = _torch()
     dim = len(nb)
-    set_launch_shape(dim, dtype, warps, chunk)
+    set_launch_shape(dim, dtype, warps, chunk, blocks)
     run = BlastRun(nb, dtype, arith=arith)
     for _ in range(warmup):
         run.step()
@@ -143,22 +147,22 @@ def tune_plain(nb, dtype, arith="strict", force=False, log=None):
     key = f"plain|{_key(dim, dtype)}|{arith}"
     if key in cache and not force:
         best = cache[key]
-        set_launch_shape(dim, dtype, best["warps"], best["chunk"])
+        set_launch_shape(dim, dtype, best["warps"], best["chunk"], best.get("blocks", 0))
         return best
     results = []
-    for w in PLAIN_WARPS[(dim, T.itemsize)]:
+    for w, b in PLAIN_SHAPES[(dim, T.itemsize)]:
         for c in PLAIN_CHUNKS[dim]:
-            rate, shape = measure_plain(nb, dtype, arith, w, c)
-            results.append((rate, w, c, shape))
+            rate, shape = measure_plain(nb, dtype, arith, w, c, b)
+            results.append((rate, w, b, c, shape))
             if log:
-                log(f"autotune {key} warps {w} chunk {c}: {rate / 1e9:.1f} GCell/s (ran {shape})")
-    rate, w, c, shape = max(results, key=lambda r: r[0])
-    best = dict(warps=w, chunk=c, gcell_s=rate / 1e9, grid=list(nb), ran=shape,
-                tried={f"{r[1]}x{r[2]}": r[0] / 1e9 for r in results})
+                log(f"autotune {key} warps {w} blocks {b} chunk {c}: {rate / 1e9:.1f} GCell/s (ran {shape})")
+    rate, w, b, c, shape = max(results, key=lambda r: r[0])
+    best = dict(warps=w, blocks=b, chunk=c, gcell_s=rate / 1e9, grid=list(nb), ran=shape,
+                tried={f"w{r[1]}_b{r[2]}_c{r[3]}": r[0] / 1e9 for r in results})
     cache[key] = best
     try:
         CACHE.write_text(json.dumps(cache, indent=1))
     except OSError:
         pass
-    set_launch_shape(dim, dtype, w, c)
+    set_launch_shape(dim, dtype, w, c, b)
     return best

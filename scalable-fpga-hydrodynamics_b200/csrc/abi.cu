@@ -297,18 +297,19 @@ int hydro_last_step_info(hydro_step_info_t *info)
 
 int hydro_device_contexts(void) { return ctx_count(); }
 
-int hydro_set_launch_shape(int dim, int precision_bytes, int warps, int chunk)
+int hydro_set_launch_shape(int dim, int precision_bytes, int warps, int chunk, int blocks_per_sm)
 {
-    return set_launch_shape(dim, (size_t)precision_bytes, warps, chunk);
+    return set_launch_shape(dim, (size_t)precision_bytes, warps, chunk, blocks_per_sm);
 }
 
-int hydro_last_launch_shape(int *warps, int *chunk, int *tma)
+int hydro_last_launch_shape(int *warps, int *chunk, int *blocks_per_sm, int *tma)
 {
     int err;
     DevCtx *c = ctx_current(&err);
     if (!c) return err;
     if (warps) *warps = c->last_warps;
     if (chunk) *chunk = c->last_chunk;
+    if (blocks_per_sm) *blocks_per_sm = c->last_blocks;
     if (tma) *tma = c->last_tma ? 1 : 0;
     return kOk;
 }

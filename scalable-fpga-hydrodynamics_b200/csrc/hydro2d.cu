@@ -117,9 +117,10 @@ template <class T, bool kF = false> __global__ void __launch_bounds__(kRedoNT) r
 
 // ------------------------------------------------------------------- strip kernel ---
 // kTma: rows staged by TMA tile loads (16-byte row pitch), else by per-lane cp.async.
-// kF: fused arithmetic (hydro_math.cuh).
-template <class T, bool kTma, bool kF>
-__global__ void __launch_bounds__(kStripNT, 4)
+// kF: fused arithmetic (hydro_math.cuh). kMinB: resident blocks per SM the registers are
+// budgeted for (a launch-shape choice: more blocks, fewer registers per thread).
+template <class T, bool kTma, bool kF, int kMinB = 4>
+__global__ void __launch_bounds__(kStripNT, kMinB)
     strip2d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args2<T> g)
 {
     __shared__ Smem2<T> S;
@@ -285,6 +286,20 @@ template <> CUtensorMapDataType tmap_type<float>() { return CU_TENSOR_MAP_DATA_T
 bool aligned(const void *p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
 } // namespace
 
+template <class T, int kMinB>
+void launch_strip2d(bool tma, bool fused, dim3 grid, cudaStream_t stream, const CUtensorMap &tmr,
+                    const CUtensorMap &tmu, const Args2<T> &g)
+{
+    if (tma && fused)
+        strip2d<T, true, true, kMinB><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
+    else if (tma)
+        strip2d<T, true, false, kMinB><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
+    else if (fused)
+        strip2d<T, false, true, kMinB><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
+    else
+        strip2d<T, false, false, kMinB><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
+}
+
 template <class T>
 int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, const Phys<T> &ph, size_t nb_x,
            size_t nb_y, T DtDx, T DtDy, cudaStream_t stream, Kernel which, bool sync, StepInfo *info, bool xwrap,
@@ -377,14 +392,13 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
         ctx->last_chunk = chunk;
         ctx->last_tma = tma_ok;
         const dim3 grid(nstrips, nchunks);
-        if (tma_ok && fused)
-            strip2d<T, true, true><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
-        else if (tma_ok)
-            strip2d<T, true, false><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
-        else if (fused)
-            strip2d<T, false, true><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
+        constexpr int kAltB = sizeof(T) == 8 ? 5 : 8; // the other register budget built
+        const bool alt = shape.blocks == kAltB;
+        ctx->last_blocks = alt ? kAltB : 4;
+        if (alt)
+            launch_strip2d<T, kAltB>(tma_ok, fused, grid, stream, tmr, tmu, g);
         else
-            strip2d<T, false, false><<<grid, kStripNT, 0, stream>>>(tmr, tmu, g);
+            launch_strip2d<T, 4>(tma_ok, fused, grid, stream, tmr, tmu, g);
     } else {
         const int gx = (int)((nb_y + kDirectNT - 1) / kDirectNT);
         const int gy = (int)std::min<size_t>(nb_x, 65535);

@@ -345,6 +345,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         }
         ctx->last_warps = W;
         ctx->last_chunk = chunk;
+        ctx->last_blocks = min_blocks3(W);
         ctx->last_tma = tma;
     } else {
         const int gx = (int)((nb_z + 31) / 32), gy = (int)((nb_y + 3) / 4), gz = (int)std::min<size_t>(nb_x, 65535);

@@ -30,6 +30,7 @@ struct DevCtx {
     int last_kernel = 0; // Kernel run by the last step launch
     int last_warps = 0;  // its launch shape (strip kernels): warps per block, rows/planes per block
     int last_chunk = 0;
+    int last_blocks = 0;   // 2D: its register budget in blocks per SM
     bool last_tma = false; // its rows/planes staged by tensor-map loads
     bool dirty = false; // a launch failed: scratch words must be re-zeroed
 };
@@ -74,11 +75,12 @@ inline unsigned long long problem_key(const void *dt_next, size_t a, size_t b, s
 // Launch shape of the plain strip kernels per (dimensionality, precision), set by
 // hydro_set_launch_shape (an autotuner); 0 fields keep the built-in choice.
 struct LaunchShape {
-    int warps = 0; // 3D: warps per block (tile rows with halo)
-    int chunk = 0; // rows (2D) or planes (3D) each block marches
+    int warps = 0;  // 3D: warps per block (tile rows with halo)
+    int chunk = 0;  // rows (2D) or planes (3D) each block marches
+    int blocks = 0; // 2D: resident blocks per SM the registers are budgeted for (4, or 5 in FP64 / 8 in FP32)
 };
 LaunchShape launch_shape(int dim, size_t tsize);
-int set_launch_shape(int dim, size_t tsize, int warps, int chunk);
+int set_launch_shape(int dim, size_t tsize, int warps, int chunk, int blocks);
 
 // Context of the current device (created on first use; never freed before exit).
 DevCtx *ctx_current(int *err);

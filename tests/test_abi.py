@@ -79,18 +79,19 @@ def test_noalloc_launch_shape_fits_the_fixed_scratch(built):
 
 
 def test_launch_shape_settings(built):
-    """hydro_set_launch_shape (host only): the tile heights the 3D kernels are built for are
-    accepted, others and 2D tile heights rejected with HYDRO_ERR_ARG; 0 restores the
-    built-in shape."""
+    """hydro_set_launch_shape (host only): the tile heights the 3D kernels are built for and
+    the 2D register budgets are accepted, anything else rejected with HYDRO_ERR_ARG; 0
+    restores the built-in shape."""
     fn = built.hydro_set_launch_shape
-    fn.argtypes = [ctypes.c_int] * 4
+    fn.argtypes = [ctypes.c_int] * 5
     fn.restype = ctypes.c_int
-    for dim, pb, w, c in ((3, 8, 8, 0), (3, 8, 12, 64), (3, 8, 16, 32), (3, 4, 8, 0), (3, 4, 16, 128),
-                          (2, 8, 0, 64), (2, 4, 0, 0)):
-        assert fn(dim, pb, w, c) == 0, (dim, pb, w, c)
-    for dim, pb, w, c in ((3, 4, 12, 0), (3, 8, 10, 0), (2, 8, 8, 0), (4, 8, 0, 0), (3, 2, 8, 0), (3, 8, 8, -1)):
-        assert fn(dim, pb, w, c) == hb.HYDRO_ERR_ARG, (dim, pb, w, c)
+    for args in ((3, 8, 8, 0, 0), (3, 8, 12, 64, 0), (3, 8, 16, 32, 0), (3, 4, 8, 0, 0), (3, 4, 16, 128, 0),
+                 (2, 8, 0, 64, 0), (2, 4, 0, 0, 0), (2, 8, 0, 0, 5), (2, 4, 0, 32, 8), (2, 8, 0, 0, 4)):
+        assert fn(*args) == 0, args
+    for args in ((3, 4, 12, 0, 0), (3, 8, 10, 0, 0), (2, 8, 8, 0, 0), (4, 8, 0, 0, 0), (3, 2, 8, 0, 0),
+                 (3, 8, 8, -1, 0), (2, 8, 0, 0, 8), (2, 4, 0, 0, 5), (3, 8, 8, 0, 4)):
+        assert fn(*args) == hb.HYDRO_ERR_ARG, args
     for dim in (2, 3):
         for pb in (4, 8):
-            assert fn(dim, pb, 0, 0) == 0
+            assert fn(dim, pb, 0, 0, 0) == 0
     built.hydro_clear_error()

@@ -303,15 +303,18 @@ def test_step_x_ghosts_from_memory(cuda, oracle, nb, T, kernel):
 
 @pytest.mark.parametrize("T", [np.float64, np.float32])
 def test_launch_shapes_bitwise(cuda, oracle, T):
-    """Every tile height and chunk the autotuner may pick gives the oracle's bits: 3D tile
-    heights (8, 12, 16 warps in FP64; 8, 16 in FP32) and explicit chunks, 2D chunks."""
+    """Every launch shape the autotuner may pick gives the oracle's bits: 3D tile heights
+    (8, 12, 16 warps in FP64; 8, 16 in FP32) with explicit chunks, 2D register budgets with
+    2D chunks."""
     warps = (8, 12, 16) if T is np.float64 else (8, 16)
-    cases = [((40, 150, 130), w, c) for w in warps for c in (0, 7, 64)] + \
-            [((9, 14, 62), w, 3) for w in warps] + [((300, 253), 0, c) for c in (0, 5, 300)]
+    alt = 5 if T is np.float64 else 8
+    cases = [((40, 150, 130), w, c, 0) for w in warps for c in (0, 7, 64)] + \
+            [((9, 14, 62), w, 3, 0) for w in warps] + \
+            [((300, 253), 0, c, b) for c in (0, 5, 300) for b in (4, alt)]
     try:
-        for nb, w, c in cases:
+        for nb, w, c, b in cases:
             phys = hb.Physics(T, nb)
-            hb.set_launch_shape(len(nb), T, w, c)
+            hb.set_launch_shape(len(nb), T, w, c, b)
             st = seeded_state(nb, T, 4)
             oracle.ghost_x(st, nb)
             ref = (np.zeros_like(st[0]), np.zeros_like(st[1]))
@@ -321,11 +324,13 @@ def test_launch_shapes_bitwise(cuda, oracle, T):
             shape = hb.last_launch_shape()
             if len(nb) == 3:
                 assert shape["warps"] == w
+            elif b:
+                assert shape["blocks"] == b
             if c:
                 assert shape["chunk"] == c
-            assert d.tobytes() == dref.tobytes(), (nb, w, c)
-            assert out[0].tobytes() == ref[0].tobytes(), (nb, w, c)
-            assert out[1].tobytes() == ref[1].tobytes(), (nb, w, c)
+            assert d.tobytes() == dref.tobytes(), (nb, w, c, b)
+            assert out[0].tobytes() == ref[0].tobytes(), (nb, w, c, b)
+            assert out[1].tobytes() == ref[1].tobytes(), (nb, w, c, b)
     finally:
         for dim in (2, 3):
-            hb.set_launch_shape(dim, T, 0, 0)
+            hb.set_launch_shape(dim, T, 0, 0, 0)
