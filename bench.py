@@ -604,7 +604,7 @@ def bench_serving_sweep(hb, torch, rates=(10.0, 30.0, 100.0, 300.0, 1000.0), nre
 
 
 # ------------------------------------------------------------------- kernel tour ---
-def bench_tour(hb, torch, hbm, reps=5, log=print):
+def bench_tour(hb, torch, hbm, reps=5, log=print, only=None):
     """Every kernel of the library on a case whose state is larger than L2 (126 MB), timed
     with CUDA events on the launching stream: one JSON line per entry with the algorithmic
     bytes of one call, its duration, GB/s and the fraction of the measured copy bandwidth.
@@ -617,6 +617,8 @@ def bench_tour(hb, torch, hbm, reps=5, log=print):
     E = torch.cuda.Event
 
     def timed(name, fn, nbytes, note="", stream=None):
+        if only and only not in name:
+            return
         st = stream or torch.cuda.current_stream()
         for _ in range(2):
             fn()
@@ -656,6 +658,11 @@ def bench_tour(hb, torch, hbm, reps=5, log=print):
             timed(f"direct{d}d<{tn}> {'x'.join(map(str, nb))}",
                   lambda: hb.step(st, nx, dt, phys, dtd, kernel=hb.KERNEL_DIRECT, sync=False),
                   cells * 2 * (2 + d) * isz, "plus the redo2d/redo3d launch, which returns at once")
+            # the strip kernels in both arithmetics (built-in launch shape)
+            for ar in ("strict", "fused"):
+                timed(f"strip{d}d<{tn}> {ar} {'x'.join(map(str, nb))}",
+                      lambda: hb.step(st, nx, dt, phys, dtd, kernel=hb.KERNEL_STRIP, sync=False, arith=ar),
+                      cells * 2 * (2 + d) * isz, "plus the redo launch, which returns at once")
             del st, nx
             torch.cuda.empty_cache()
         # the exact signal-speed pass: a calm state stepped after a fast one on the same
@@ -740,6 +747,7 @@ def main():
                     help="the serving workload as configured (rates 10..1000/s, 200 requests each, plus a "
                          "budget-bound stream) instead of the plain-path benchmark; one JSON line")
     ap.add_argument("--serving-trace", default=None, help="file for the sweep's request traces")
+    ap.add_argument("--tour-only", default=None, help="with --tour: only the entries whose name contains this")
     ap.add_argument("--tour", action="store_true",
                     help="time every kernel of the library on a small case (one JSON line each) and exit")
     args = ap.parse_args()
@@ -808,7 +816,7 @@ def main():
         return
     if args.tour:
         if rank == 0:
-            bench_tour(hb, torch, hbm, log=lambda m: print(m, flush=True))
+            bench_tour(hb, torch, hbm, log=lambda m: print(m, flush=True), only=args.tour_only)
         reps.barrier()
         reps.close()
         return
