@@ -77,7 +77,7 @@ def test_write_csv_matches_reference_program(cuda, prog, nb, T, steps, tmp_path)
     ref = _reference_csv(prog, dims + ["-t", "100", "-i", str(steps), "-w", str(steps)], tmp_path)
     files = sorted(ref.glob(f"output_{steps}_*.csv"))
     assert len(files) == 1, list(ref.iterdir())
-    run = hb.BlastRun(nb, T).run(1e9, steps)
+    run = hb.BlastRun(nb, T, arith="strict").run(1e9, steps)
     out = tmp_path / "gpu.csv"
     n = hb.write_csv(run.cur, nb, out)
     data = out.read_bytes()
@@ -94,7 +94,7 @@ def test_write_csv_many_chunks(cuda, chunk_cells, tmp_path, monkeypatch):
     ref = _reference_csv("hydro", ["-x", "200", "-y", "150", "-t", "100", "-i", str(steps), "-w", str(steps)],
                          tmp_path)
     files = sorted(ref.glob(f"output_{steps}_*.csv"))
-    run = hb.BlastRun(nb, np.float64).run(1e9, steps)
+    run = hb.BlastRun(nb, np.float64, arith="strict").run(1e9, steps)
     monkeypatch.setenv("HYDRO_B200_CSV_CHUNK_CELLS", str(chunk_cells))
     out = tmp_path / "gpu.csv"
     hb.write_csv(run.cur, nb, out)

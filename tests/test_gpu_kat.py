@@ -23,7 +23,7 @@ def test_kat_full_run(cuda, kat, name):
     log = kat[name]
     cfg = log["config"]
     nb = (cfg["nb_x"], cfg["nb_y"]) + ((cfg["nb_z"],) if "nb_z" in cfg else ())
-    run = hb.BlastRun(nb, np.float64)
+    run = hb.BlastRun(nb, np.float64, arith="strict")
     assert "%.7e" % run.mass0 == log["initial_mass"]
     assert "%.2e" % run.first_dt == log["initial_dt"]
     run.run(cfg["max_t"], cfg["max_it"])

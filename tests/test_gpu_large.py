@@ -117,7 +117,7 @@ def _check_step(oracle, phys, dtd, nb, before, after, dt_dev, info, slab_rows):
 @pytest.mark.parametrize("T", [np.float64, np.float32])
 @pytest.mark.parametrize("nb,slab_rows", [((40000, 20000), 200), ((512, 512, 512), 16)])
 def test_large_grid_steps_match_oracle(cuda, oracle, nb, slab_rows, T):
-    run = hb.BlastRun(nb, T)
+    run = hb.BlastRun(nb, T, arith="strict")
     phys = run.phys
     # the device initial condition: mass and first Dt against the oracle's statistics
     m0, dt0 = oracle.blast_stats(nb, phys)

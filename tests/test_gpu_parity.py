@@ -85,7 +85,7 @@ def test_golden_runs(cuda, orc, ref_runs, kernel):
     meta, arrays = ref_runs
     for name, m in meta.items():
         T = np.dtype(m["dtype"]).type
-        run = hb.BlastRun(tuple(m["nb"]), T, kernel=kernel).run(m["max_t"], m["max_it"])
+        run = hb.BlastRun(tuple(m["nb"]), T, kernel=kernel, arith="strict").run(m["max_t"], m["max_it"])
         assert float(run.first_dt) == m["first_dt"], name
         assert run.it == m["it"], name
         assert np.array_equal(np.array(run.t_log), arrays[name + "__t"]), name
@@ -112,7 +112,7 @@ def test_speed_skip_redo_is_exact(cuda, oracle, nb):
             for st in (fast, calm):
                 cur = to_dev(cuda, st)
                 nxt = tuple(cuda.zeros_like(a) for a in cur)
-                hb.step(cur, nxt, dt, phys, dtd, kernel=kernel, sync=sync)
+                hb.step(cur, nxt, dt, phys, dtd, kernel=kernel, sync=sync, arith="strict")
                 cuda.cuda.synchronize()
                 ref = (np.zeros_like(st[0]), np.zeros_like(st[1]))
                 dref = oracle.step(st, ref, phys, dtd)
@@ -124,13 +124,13 @@ def test_strip_equals_direct_large(cuda):
     """Strip and direct kernels on a grid with many strips and chunks."""
     nb = (1500, 1000)
     for T in (np.float64, np.float32):
-        a = hb.BlastRun(nb, T, kernel=hb.KERNEL_STRIP).run(1.0, 25)
+        a = hb.BlastRun(nb, T, kernel=hb.KERNEL_STRIP, arith="strict").run(1.0, 25)
         b = hb.BlastRun(nb, T, kernel=hb.KERNEL_DIRECT).run(1.0, 25)
         assert a.dt_log == b.dt_log
         sa, sb = a.host_state(), b.host_state()
         assert sa[0].tobytes() == sb[0].tobytes() and sa[1].tobytes() == sb[1].tobytes()
     nb3 = (70, 64, 62)
-    a = hb.BlastRun(nb3, np.float64, kernel=hb.KERNEL_STRIP).run(1.0, 10)
+    a = hb.BlastRun(nb3, np.float64, kernel=hb.KERNEL_STRIP, arith="strict").run(1.0, 10)
     b = hb.BlastRun(nb3, np.float64, kernel=hb.KERNEL_DIRECT).run(1.0, 10)
     assert a.dt_log == b.dt_log
     assert digest(a.host_state()) == digest(b.host_state())
@@ -294,7 +294,7 @@ def test_step_x_ghosts_from_memory(cuda, oracle, nb, T, kernel):
         dt = cuda.zeros(1, dtype=cur[0].dtype, device="cuda")
         if kernel == hb.KERNEL_STRIP and len(nb) == 2 and T is np.float32 and (nb[1] + 2) % 2:
             continue
-        _, info = hb.step(cur, nxt, dt, phys, dtd, kernel=kernel, x_ghosts=True)
+        _, info = hb.step(cur, nxt, dt, phys, dtd, kernel=kernel, x_ghosts=True, arith="strict")
         assert info.kernel == kernel
         assert phys.dtype(dt.item()).tobytes() == dref.tobytes()
         out = tuple(a.cpu().numpy() for a in nxt)

@@ -83,7 +83,7 @@ def test_noalloc_step_matches_regular_step_twice(cuda, nb):
         ia, ib = hb.StepInfo(), hb.StepInfo()
         rc = L.hydro2d_step_f64(hb._ptr(cur_a[0]), hb._ptr(cur_a[1]), hb._ptr(nxt_a[0]), hb._ptr(nxt_a[1]),
                                 hb._ptr(dt_a), phys.C_min, phys.g, phys.gm1, phys.divgamma, phys.k, nb[0], nb[1],
-                                dtd[0], dtd[1], stream, 0, 1, ctypes.byref(ia))
+                                dtd[0], dtd[1], stream, hb.ARITH_STRICT, 1, ctypes.byref(ia))
         assert rc == 0, hb.last_error()
         rc = noalloc(hb._ptr(cur_b[0]), hb._ptr(cur_b[1]), hb._ptr(nxt_b[0]), hb._ptr(nxt_b[1]), hb._ptr(dt_b),
                      phys.C_min, phys.g, phys.gm1, phys.divgamma, phys.k, nb[0], nb[1], dtd[0], dtd[1], stream, 1,
