@@ -403,8 +403,7 @@ __global__ void __launch_bounds__(kStripNT, Batch2dOcc<T>::value) batch2d(Inst2<
         const bool ok = march2d<T, true, kF>(S, &I->tm[par][0], &I->tm[par][1], geo, I->rhoE[par ^ 1], I->uv[par ^ 1], ph,
                                    I->DtDx, I->DtDy, ld, [&](const Upd2<T> &o) {
                                        if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
-                                       const float fu = (float)o.u, fv = (float)o.v;
-                                       if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1, tlo2))
+                                       if (!state_below(o, ggm1, tlo2))
                                            acc.add_speed((double)speed2<T, kF>(o.r, o.u, o.v, o.E, ph));
                                    });
         if (!ok) acc.err |= kErrWaitTimeout;
@@ -444,8 +443,7 @@ __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) batch3d(Inst3<T> *ins
         march3d<T, kF>(S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy,
                    I->DtDz, [&](const Upd3<T> &o) {
                        if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
-                       const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
-                       if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1, tlo2))
+                       if (!state_below(o, ggm1, tlo2))
                            acc.add_speed((double)speed3<T, kF>(o.r, o.u, o.v, o.w, o.E, ph));
                    });
         const int2 rg = ranges[it.x];

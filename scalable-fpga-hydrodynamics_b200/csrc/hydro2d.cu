@@ -140,8 +140,7 @@ __global__ void __launch_bounds__(kStripNT, kMinB)
     const bool ok = march2d<T, kTma, kF>(S, &tmr, &tmu, geo, g.rhoE_n, g.uv_n, ph, g.DtDx, g.DtDy, ld,
                                          [&](const Upd2<T> &o) {
                                              acc.add_mass(o.r);
-                                             const float fu = (float)o.u, fv = (float)o.v;
-                                             if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv, ggm1, tlo2))
+                                             if (!state_below(o, ggm1, tlo2))
                                                  acc.add_speed(speed2<T, kF>(o.r, o.u, o.v, o.E, ph));
                                          });
     if (!ok) acc.err |= kErrWaitTimeout;

@@ -133,8 +133,7 @@ __global__ void __launch_bounds__(32 * W, min_blocks3(W))
         S, g.rhoE, g.uvw, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz,
         [&](const Upd3<T> &o) {
             acc.add_mass(o.r);
-            const float fu = (float)o.u, fv = (float)o.v, fw = (float)o.w;
-            if (!speed_below((float)o.r, (float)o.E, fu * fu + fv * fv + fw * fw, ggm1, tlo2))
+            if (!state_below(o, ggm1, tlo2))
                 acc.add_speed(speed3<T, kF>(o.r, o.u, o.v, o.w, o.E, ph));
         },
         Tmaps3{&tmr, &tmu});

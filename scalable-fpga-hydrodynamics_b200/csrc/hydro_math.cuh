@@ -355,6 +355,23 @@ __device__ __forceinline__ bool speed_below(float r, float E, float m2, float gg
     if (!(r > 1e-6f) || !(r < 1e6f) || !(E > 1e-6f) || !(E < 1e12f) || !(m2 < 1e24f)) return false;
     return (ggm1 * E * r + m2) * (2.0f * (1.0f + 1.0f / 4096.0f)) < tlo2 * (r * r);
 }
+// The same test in FP64 for FP64 states (no conversions; the same bound, ranges and margin).
+__device__ __forceinline__ bool speed_below(double r, double E, double m2, double ggm1, double tlo2)
+{
+    if (!(r > 1e-6) || !(r < 1e6) || !(E > 1e-6) || !(E < 1e12) || !(m2 < 1e24)) return false;
+    return (ggm1 * E * r + m2) * (2.0 * (1.0 + 1.0 / 4096.0)) < tlo2 * (r * r);
+}
+// The skip test of a new 2D / 3D state in the state's own precision.
+template <class T> __device__ __forceinline__ bool state_below(const Upd2<T> &o, float ggm1, float tlo2)
+{
+    return speed_below(o.r, o.E, o.u * o.u + o.v * o.v, (T)ggm1, (T)tlo2);
+}
+template <class T> struct Upd3;
+template <class T> __device__ __forceinline__ bool state_below(const Upd3<T> &o, float ggm1, float tlo2)
+{
+    return speed_below(o.r, o.E, o.u * o.u + o.v * o.v + o.w * o.w, (T)ggm1, (T)tlo2);
+}
+
 // tlo^2 for speed_below; 0 (nothing skips) above the range the test is safe for
 __device__ __forceinline__ float skip_tlo2(float tlof) { return (tlof <= 1e6f) ? tlof * tlof : 0.0f; }
 // gamma (gamma - 1) in FP32 for speed_below; +inf (nothing skips) unless gamma > 1

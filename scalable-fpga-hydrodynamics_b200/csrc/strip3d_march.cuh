@@ -72,9 +72,14 @@ template <class T, int NT> __device__ __forceinline__ FaceIn3<T> xp_face_y(const
     const auto q0 = x[0 * NT], q1 = x[1 * NT], q2 = x[2 * NT], q3 = x[3 * NT], q4 = x[4 * NT];
     return FaceIn3<T>{q0.x, q2.x, q0.y, q1.x, q1.y, q3.y, q3.x, q4.x, q4.y}; // normal v: (v, u, w)
 }
-template <class T, int NT> __device__ __forceinline__ FaceIn3<T> xp_face_z(const typename Vec2<T>::type *x)
+// (in fused arithmetic the z faces take the same upwinded energy as x and y faces, so
+// the sixth pair is neither published nor read)
+template <class T, int NT, bool kF = false>
+__device__ __forceinline__ FaceIn3<T> xp_face_z(const typename Vec2<T>::type *x)
 {
-    const auto q0 = x[0 * NT], q1 = x[1 * NT], q2 = x[2 * NT], q3 = x[3 * NT], q4 = x[4 * NT], q5 = x[5 * NT];
+    const auto q0 = x[0 * NT], q1 = x[1 * NT], q2 = x[2 * NT], q3 = x[3 * NT], q4 = x[4 * NT];
+    if constexpr (kF) return FaceIn3<T>{q0.x, q2.y, q0.y, q1.x, q1.y, q4.x, q3.y, q3.x, q4.y};
+    const auto q5 = x[5 * NT];
     return FaceIn3<T>{q0.x, q2.y, q0.y, q1.x, q1.y, q4.x, q3.y, q3.x, q5.x}; // normal w: (w, v, u)
 }
 
@@ -228,7 +233,7 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T, W> &S, const T *rhoE, cons
             x[2 * (32 * W)] = pair3<T>(P.v, P.w);
             x[3 * (32 * W)] = pair3<T>(P.mu, P.mv);
             x[4 * (32 * W)] = pair3<T>(P.mw, P.eup_xy);
-            x[5 * (32 * W)] = pair3<T>(P.eup_z, T(0));
+            if constexpr (!kF) x[5 * (32 * W)] = pair3<T>(P.eup_z, T(0));
         }
         // +y face of (j | j+1), from this lane's previous-plane cell and the warp above's
         auto yface = [&]() {
@@ -245,7 +250,7 @@ __device__ __forceinline__ bool march3d_tile(Smem3<T, W> &S, const T *rhoE, cons
         // reads the next warp's lane 0, a face no interior lane uses)
         auto zface = [&]() {
             const FaceIn3<T> mz = face3_z(Pm);
-            const FaceIn3<T> nz = xp_face_z<T, 32 * W>(&S.xP[(m - 1) & 1][0][t + 1]);
+            const FaceIn3<T> nz = xp_face_z<T, 32 * W, kF>(&S.xP[(m - 1) & 1][0][t + 1]);
             FaceIn3<T> L = mz, R = nz;
             if (kEdge) {
                 if (k == 0) L = mirror3(nz);
