@@ -116,13 +116,11 @@ PLAIN_SHAPES = {(2, 4): [(0, 4), (0, 8)], (2, 8): [(0, 4), (0, 5)], (3, 4): [(8,
 PLAIN_CHUNKS = {2: (0, 32, 64, 128, 256), 3: (0, 16, 32, 64, 128)}
 
 
-def measure_plain(nb, dtype, arith, warps, chunk, blocks=0, steps=4, warmup=2):
-    """Cell-updates per second of the plain path with one launch shape (CUDA events around
-    `steps` steps after `warmup`), on the blast of grid `nb`."""
+def measure_plain(run, warps, chunk, blocks=0, steps=3, warmup=1):
+    """Cell-updates per second of the plain path with one launch shape: CUDA events around
+    `steps` steps of `run` (a BlastRun) after `warmup`, and the shape that ran."""
     torch = _torch()
-    dim = len(nb)
-    set_launch_shape(dim, dtype, warps, chunk, blocks)
-    run = BlastRun(nb, dtype, arith=arith)
+    set_launch_shape(len(run.nb), run.T, warps, chunk, blocks)
     for _ in range(warmup):
         run.step()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -132,15 +130,14 @@ def measure_plain(nb, dtype, arith, warps, chunk, blocks=0, steps=4, warmup=2):
         run.step()
     e1.record()
     torch.cuda.synchronize()
-    shape = last_launch_shape()
-    del run
-    torch.cuda.empty_cache()
-    return int(np.prod(nb)) * steps / (e0.elapsed_time(e1) / 1e3), shape
+    return int(np.prod(run.nb)) * steps / (e0.elapsed_time(e1) / 1e3), last_launch_shape()
 
 
 def tune_plain(nb, dtype, arith="strict", force=False, log=None):
-    """The fastest (warps, chunk) of the plain path for (this GPU, dim, dtype, arith), timed
-    on grid `nb` once and then cached; installs it and returns it as a dict."""
+    """The fastest launch shape of the plain path for (this GPU, dim, dtype, arith), timed
+    on the blast of grid `nb` once and then cached; installs it and returns it as a dict.
+    One run steps through every candidate twice, in opposite orders (the state evolves
+    between candidates), and each candidate keeps its faster pass."""
     dim = len(nb)
     T = np.dtype(dtype)
     cache = _load()
@@ -149,16 +146,23 @@ def tune_plain(nb, dtype, arith="strict", force=False, log=None):
         best = cache[key]
         set_launch_shape(dim, dtype, best["warps"], best["chunk"], best.get("blocks", 0))
         return best
-    results = []
-    for w, b in PLAIN_SHAPES[(dim, T.itemsize)]:
-        for c in PLAIN_CHUNKS[dim]:
-            rate, shape = measure_plain(nb, dtype, arith, w, c, b)
-            results.append((rate, w, b, c, shape))
-            if log:
-                log(f"autotune {key} warps {w} blocks {b} chunk {c}: {rate / 1e9:.1f} GCell/s (ran {shape})")
-    rate, w, b, c, shape = max(results, key=lambda r: r[0])
-    best = dict(warps=w, blocks=b, chunk=c, gcell_s=rate / 1e9, grid=list(nb), ran=shape,
-                tried={f"w{r[1]}_b{r[2]}_c{r[3]}": r[0] / 1e9 for r in results})
+    torch = _torch()
+    cands = [(w, b, c) for w, b in PLAIN_SHAPES[(dim, T.itemsize)] for c in PLAIN_CHUNKS[dim]]
+    run = BlastRun(nb, np.dtype(dtype).type, arith=arith)
+    rates, shapes = {}, {}
+    for order in (cands, cands[::-1]):
+        for w, b, c in order:
+            rate, shape = measure_plain(run, w, c, b)
+            rates[(w, b, c)] = max(rates.get((w, b, c), 0.0), rate)
+            shapes[(w, b, c)] = shape
+    del run
+    torch.cuda.empty_cache()
+    if log:
+        for (w, b, c), r in rates.items():
+            log(f"autotune {key} warps {w} blocks {b} chunk {c}: {r / 1e9:.1f} GCell/s (ran {shapes[(w, b, c)]})")
+    (w, b, c), rate = max(rates.items(), key=lambda kv: kv[1])
+    best = dict(warps=w, blocks=b, chunk=c, gcell_s=rate / 1e9, grid=list(nb), ran=shapes[(w, b, c)],
+                tried={f"w{k[0]}_b{k[1]}_c{k[2]}": v / 1e9 for k, v in rates.items()})
     cache[key] = best
     try:
         CACHE.write_text(json.dumps(cache, indent=1))
