@@ -617,7 +617,7 @@ def bench_tour(hb, torch, hbm, reps=5, log=print, only=None):
     E = torch.cuda.Event
 
     def timed(name, fn, nbytes, note="", stream=None):
-        if only and only not in name:
+        if only and only not in name.replace(" ", "_"):
             return
         st = stream or torch.cuda.current_stream()
         for _ in range(2):
@@ -747,7 +747,8 @@ def main():
                     help="the serving workload as configured (rates 10..1000/s, 200 requests each, plus a "
                          "budget-bound stream) instead of the plain-path benchmark; one JSON line")
     ap.add_argument("--serving-trace", default=None, help="file for the sweep's request traces")
-    ap.add_argument("--tour-only", default=None, help="with --tour: only the entries whose name contains this")
+    ap.add_argument("--tour-only", default=None,
+                    help="with --tour: only the entries whose name (spaces as underscores) contains this")
     ap.add_argument("--tour", action="store_true",
                     help="time every kernel of the library on a small case (one JSON line each) and exit")
     args = ap.parse_args()
