@@ -747,6 +747,8 @@ def main():
                     help="the serving workload as configured (rates 10..1000/s, 200 requests each, plus a "
                          "budget-bound stream) instead of the plain-path benchmark; one JSON line")
     ap.add_argument("--serving-trace", default=None, help="file for the sweep's request traces")
+    ap.add_argument("--serving-bound-requests", type=int, default=2000,
+                    help="requests of the sweep's budget-bound stream (0: none)")
     ap.add_argument("--tour-only", default=None,
                     help="with --tour: only the entries whose name (spaces as underscores) contains this")
     ap.add_argument("--tour", action="store_true",
@@ -810,6 +812,7 @@ def main():
         if rank == 0:
             sw = bench_serving_sweep(hb, torch, rates=tuple(args.serving_rates), nreq=args.serving_requests,
                                      plain=not args.no_serving_plain, trace_path=args.serving_trace,
+                                     bound_requests=args.serving_bound_requests,
                                      log=lambda m: print(m, file=sys.stderr, flush=True))
             print(json.dumps(dict(serving_sweep=sw)), flush=True)
         reps.barrier()
