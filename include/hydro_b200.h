@@ -198,8 +198,9 @@ unsigned hydro2d_noalloc_launch_shape(size_t NB_X, size_t NB_Y, int strip, int s
  * autotuner picks it. 0 keeps the built-in choice for any field.
  *  warps: 3D only, warps per block, i.e. tile rows with the one-row halo (8, 16, and 12 in
  *    FP64; built-in 8 in FP64, 16 in FP32);
- *  chunk: rows (2D) or planes (3D) each block marches (built-in: sized from the grid and
- *    the SM count);
+ *  chunk: the most rows (2D) or planes (3D) one block marches (built-in 256); blocks take
+ *    fewer on grids too small to fill the GPU with that many (sized from the grid and the
+ *    SM count);
  *  blocks_per_sm: 2D only, the resident blocks per SM the kernel's registers are budgeted
  *    for (4, or 5 in FP64 / 8 in FP32; built-in 4).
  * Process-wide; the results do not depend on the shape. No counterpart in the reference,

@@ -1,9 +1,9 @@
 """Tile-shape autotuner, keyed on dimensionality and precision.
 
 Plain path (`tune_plain`): the strip kernels take two shape parameters each. Both take the
-number of X rows (2D) or planes (3D) each block marches (`chunk`, or 0 for the built-in
-size from the grid and the SM count): longer chunks re-read fewer halo rows but give fewer
-blocks. The 3D kernel also takes its tile height (warps per block, i.e. tile rows with the
+most X rows (2D) or planes (3D) one block marches (`chunk`, 0 for the built-in 256; grids
+too small to fill the GPU with such blocks take fewer, so a value tuned on one grid suits
+others): longer chunks re-read fewer halo rows but give fewer blocks. The 3D kernel also takes its tile height (warps per block, i.e. tile rows with the
 one-row halo: 8, 12 or 16 in FP64, 8 or 16 in FP32): taller tiles recompute fewer halo
 rows but hold one block per SM. The 2D kernel also takes its register budget in resident
 blocks per SM (4, or 5 in FP64 / 8 in FP32): more resident warps against fewer registers

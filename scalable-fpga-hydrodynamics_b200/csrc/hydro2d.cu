@@ -366,18 +366,15 @@ int step2d(const T *rhoE, const T *uv, T *rhoE_next, T *uv_next, T *Dt_next, con
     unsigned nblocks;
     if (use_strip) {
         const int nstrips = (int)((nb_y + kStripW - 1) / kStripW);
-        // rows per block: the tuned value when one is set (hydro_set_launch_shape), else
-        // sized for about 24 blocks per SM
+        // rows per block: sized for about 24 blocks per SM, at least 16 and at most the cap
+        // (the tuned value when one is set with hydro_set_launch_shape, else 256), so that
+        // small grids still fill the GPU
         const LaunchShape shape = launch_shape(2, sizeof(T));
-        int nchunks, chunk;
-        if (shape.chunk > 0) {
-            chunk = shape.chunk;
-        } else {
-            const int target = device_sms() * 3 * 8;
-            nchunks = (target + nstrips - 1) / nstrips;
-            chunk = (int)((nb_x + nchunks - 1) / nchunks);
-            chunk = std::min(256, std::max(16, chunk));
-        }
+        const int cap = shape.chunk > 0 ? shape.chunk : 256;
+        const int target = device_sms() * 3 * 8;
+        int nchunks = (target + nstrips - 1) / nstrips;
+        int chunk = (int)((nb_x + nchunks - 1) / nchunks);
+        chunk = std::min(cap, std::max(std::min(16, cap), chunk));
         nchunks = (int)((nb_x + chunk - 1) / chunk);
         if (nchunks > 65535) {
             chunk = (int)((nb_x + 65534) / 65535);

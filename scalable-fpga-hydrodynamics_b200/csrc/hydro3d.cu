@@ -293,15 +293,13 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
             set_error(kErrArg, "step3d: NB_Y %zu too large for the strip kernel", nb_y);
             return kErrArg;
         }
-        int nchunks, chunk;
-        if (shape.chunk > 0) {
-            chunk = shape.chunk;
-        } else {
-            const int target = device_sms() * min_blocks3(W) * 8;
-            nchunks = std::max(1, (target + nz * ny - 1) / (nz * ny));
-            chunk = (int)((nb_x + nchunks - 1) / nchunks);
-            chunk = std::min(256, std::max(8, chunk));
-        }
+        // planes per block: sized for about 8 waves of resident blocks, at least 8 and at
+        // most the cap (the tuned value when one is set, else 256)
+        const int cap = shape.chunk > 0 ? shape.chunk : 256;
+        const int target = device_sms() * min_blocks3(W) * 8;
+        int nchunks = std::max(1, (target + nz * ny - 1) / (nz * ny));
+        int chunk = (int)((nb_x + nchunks - 1) / nchunks);
+        chunk = std::min(cap, std::max(std::min(8, cap), chunk));
         nchunks = (int)((nb_x + chunk - 1) / chunk);
         if (nchunks > 65535) {
             chunk = (int)((nb_x + 65534) / 65535);
