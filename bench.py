@@ -349,10 +349,11 @@ def cpu_reference_sample(nb_y: int, rows: int, seconds: float, threads: int):
 # --------------------------------------------------------------- batched / serving ---
 def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=0, log=print, meter=None):
     """The batched workload (256 seeded 2D blasts, sides log-uniform in [64, 2048], 200
-    steps each) through the FP32 and FP64 batch engines (chunk from the autotuner), and the
-    same instances one at a time through the plain FP64 path. Accuracy: FP32 against the
-    FP64 batch (bit-identical to the plain FP64 path) on every instance. `chunk` > 0 fixes
-    the rows per work item instead of asking the autotuner."""
+    steps each) through the FP32 batch engine in fused and in strict arithmetic and the FP64
+    engine in strict arithmetic (chunk from the autotuner), and the same instances one at a
+    time through the plain FP64 path. Accuracy: each FP32 run against the FP64 batch
+    (bit-identical to the plain FP64 path) on every instance. `chunk` > 0 fixes the rows per
+    work item instead of asking the autotuner."""
     from hydro_b200.autotune import tune
     from hydro_b200.batch import Batch
     from hydro_b200.workloads import batch_blasts
@@ -361,16 +362,16 @@ def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=
     blasts = batch_blasts(n, seed=seed, steps=steps)
     cells = sum(int(np.prod(b.nb)) for b in blasts)
     states = {}
-    for T in (np.float32, np.float64):
+    for T, ar in ((np.float32, "fused"), (np.float32, "strict"), (np.float64, "strict")):
         ck = chunk if chunk > 0 else tune(2, T, log=log)
         s = torch.cuda.Stream()
         # warm-up: a throw-away batch of the same instances runs a few steps
-        w = Batch(2, T, chunk=ck, capacity=n, stream=s)
+        w = Batch(2, T, chunk=ck, capacity=n, stream=s, arith=ar)
         for bl in blasts[:32]:
             w.add(bl)
         w.run(3)
         w.close()
-        b = Batch(2, T, chunk=ck, capacity=n, stream=s)
+        b = Batch(2, T, chunk=ck, capacity=n, stream=s, arith=ar)
         slots = [b.add(bl) for bl in blasts]
         b.prepare(steps)  # graph captured and instantiated outside the timed region
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -386,8 +387,8 @@ def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=
         ms = e0.elapsed_time(e1)
         done = sum(b.status(k)["steps"] for k in slots)
         assert done == n * steps, (done, n * steps)
-        key = "fp32" if T is np.float32 else "fp64"
-        out[f"batched_{key}"] = dict(value=cells * steps / (ms / 1e3) / 1e9, unit=UNIT, ms=ms, wall_s=wall,
+        key = ("fp32" if T is np.float32 else "fp64") + ("_fused" if ar == "fused" else "")
+        out[f"batched_{key}"] = dict(arith=ar, value=cells * steps / (ms / 1e3) / 1e9, unit=UNIT, ms=ms, wall_s=wall,
                                      chunk=ck, instances=n, steps=steps, cells=cells,
                                      bytes_per_cell=32 if T is np.float32 else 64,
                                      energy=energy_entry(None if j0 is None or j1 is None else j1 - j0, wall,
@@ -395,16 +396,17 @@ def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=
         states[key] = [b.state(k)[0] for k in slots]
         b.close()
     # accuracy of the FP32 batch against FP64 (rho, relative L1 and L-inf per instance)
-    l1, linf = [], []
-    for a, r, bl in zip(states["fp32"], states["fp64"], blasts):
-        sh = tuple(x + 2 for x in bl.nb) + (2,)
-        inner = tuple(slice(1, x + 1) for x in bl.nb)
-        ra = a.reshape(sh)[inner][..., 0].astype(np.float64)
-        rr = r.reshape(sh)[inner][..., 0]
-        l1.append(np.abs(ra - rr).sum() / np.abs(rr).sum())
-        linf.append(np.abs(ra - rr).max() / np.abs(rr).max())
-    out["batched_fp32"]["rho_rel_l1_vs_fp64_max"] = float(max(l1))
-    out["batched_fp32"]["rho_rel_linf_vs_fp64_max"] = float(max(linf))
+    for key in ("fp32", "fp32_fused"):
+        l1, linf = [], []
+        for a, r, bl in zip(states[key], states["fp64"], blasts):
+            sh = tuple(x + 2 for x in bl.nb) + (2,)
+            inner = tuple(slice(1, x + 1) for x in bl.nb)
+            ra = a.reshape(sh)[inner][..., 0].astype(np.float64)
+            rr = r.reshape(sh)[inner][..., 0]
+            l1.append(np.abs(ra - rr).sum() / np.abs(rr).sum())
+            linf.append(np.abs(ra - rr).max() / np.abs(rr).max())
+        out[f"batched_{key}"]["rho_rel_l1_vs_fp64_max"] = float(max(l1))
+        out[f"batched_{key}"]["rho_rel_linf_vs_fp64_max"] = float(max(linf))
     # plain FP64 path, one instance at a time (the reference host loop per instance)
     sample = blasts if plain_sample is None else blasts[:plain_sample]
     pcells = sum(int(np.prod(b.nb)) for b in sample)
@@ -417,6 +419,8 @@ def bench_batched(hb, torch, n=256, steps=200, seed=0, plain_sample=None, chunk=
     out["plain_fp64_one_at_a_time"] = dict(value=pcells * steps / pw / 1e9, unit=UNIT, wall_s=pw,
                                            instances=len(sample), steps=steps)
     out["batched_fp32_over_plain_fp64"] = out["batched_fp32"]["value"] / out["plain_fp64_one_at_a_time"]["value"]
+    out["batched_fp32_fused_over_plain_fp64"] = (out["batched_fp32_fused"]["value"]
+                                                 / out["plain_fp64_one_at_a_time"]["value"])
     return out
 
 
@@ -434,7 +438,7 @@ def bench_serving(hb, torch, rates=(10.0, 100.0, 1000.0), nreq=8, seed=0, max_wa
 
     def served(reqs, dtype=None):
         srv = Server(hbm_budget=150e9, steps_per_tick=8, chunk2d=best_chunk(2, np.float32),
-                     chunk3d=best_chunk(3, np.float32))
+                     chunk3d=best_chunk(3, np.float32), arith={np.float32: "fused"})
         recs, wall = srv.serve(reqs, max_wall=max_wall, dtype=dtype)
         srv.close()
         torch.cuda.empty_cache()
@@ -561,7 +565,7 @@ def bench_serving_sweep(hb, torch, rates=(10.0, 30.0, 100.0, 300.0, 1000.0), nre
 
     def served(reqs, budget=150e9, wall_cap=max_wall):
         srv = Server(hbm_budget=budget, steps_per_tick=8, chunk2d=best_chunk(2, np.float32),
-                     chunk3d=best_chunk(3, np.float32))
+                     chunk3d=best_chunk(3, np.float32), arith={np.float32: "fused"})
         recs, wall = srv.serve(reqs, max_wall=wall_cap)
         stats = dict(srv.stats)
         srv.close()
@@ -939,10 +943,12 @@ def main():
         # the metric's own quantities, compact, ahead of the detailed records
         if batched:
             line["batched_fp32_gcell_s"] = batched["batched_fp32"]["value"]
+            line["batched_fp32_fused_gcell_s"] = batched["batched_fp32_fused"]["value"]
             line["batched_fp64_gcell_s"] = batched["batched_fp64"]["value"]
             line["batched_fp32_over_plain_fp64_same_instances"] = batched["batched_fp32_over_plain_fp64"]
             line["batched_fp32_over_plain_fp64_large_grid"] = batched["batched_fp32"]["value"] / value
             line["batched_fp32_rho_rel_l1_vs_fp64"] = batched["batched_fp32"]["rho_rel_l1_vs_fp64_max"]
+            line["batched_fp32_fused_rho_rel_l1_vs_fp64"] = batched["batched_fp32_fused"]["rho_rel_l1_vs_fp64_max"]
         if serving:
             top = serving[max(serving, key=lambda k: float(k.split("_")[1]))]
             line["serving"] = {k: dict(p50_s=v["batched"]["p50_s"], p99_s=v["batched"]["p99_s"],

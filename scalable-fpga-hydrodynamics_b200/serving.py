@@ -57,7 +57,9 @@ class Server:
     """Continuous batching over batch engines keyed by (dim, precision)."""
 
     def __init__(self, hbm_budget: float = 150e9, steps_per_tick: int = 8, chunk2d: int = 0, chunk3d: int = 0,
-                 capacity: int = 4096):
+                 capacity: int = 4096, arith: dict = None):
+        """arith: the arithmetic of the engines per precision, e.g. {np.float32: "fused"}
+        (missing precisions: the library default)."""
         self.torch = _torch()
         self.budget = float(hbm_budget)
         self.steps_per_tick = int(steps_per_tick)
@@ -66,13 +68,15 @@ class Server:
         self.engines = {}
         self.streams = {}
         self.stats = {}
+        self.arith = {np.dtype(k).name: v for k, v in (arith or {}).items()}
 
     def engine(self, dim, dtype) -> Batch:
         key = (dim, np.dtype(dtype).name)
         if key not in self.engines:
             s = self.torch.cuda.Stream()
             self.streams[key] = s
-            self.engines[key] = Batch(dim, dtype, chunk=self.chunks[dim], capacity=self.capacity, stream=s)
+            self.engines[key] = Batch(dim, dtype, chunk=self.chunks[dim], capacity=self.capacity, stream=s,
+                                      arith=self.arith.get(np.dtype(dtype).name))
         return self.engines[key]
 
     def close(self):
