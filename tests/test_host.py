@@ -386,3 +386,29 @@ def test_slab_schedule_gloo_matches_whole_domain(world, nb, overlap):
         assert got.tobytes() == np.ascontiguousarray(want[k]).tobytes()
     for rank, lo, hi, _, t, dt in out:
         assert t == t_log[-1] + float(dt_log[-1]) and dt == float(dt_log[-1])
+
+
+def test_serving_stream_matches_saved_trace():
+    """The serving workload's seeded request stream (the one the serving sweep ran) is
+    regenerated exactly: grids, blast parameters, end times, precisions and arrivals of
+    the saved trace, and the streams at other rates are the same requests with scaled
+    arrivals."""
+    import json
+
+    from conftest import GOLDEN
+
+    load_pkg()
+    from hydro_b200.workloads import request_stream
+
+    saved = json.loads((GOLDEN / "serving_trace.json").read_text())
+    reqs = request_stream(saved["rate"], seed=saved["seed"], count=saved["count"])
+    assert len(reqs) == len(saved["requests"])
+    for r, s in zip(reqs, saved["requests"]):
+        assert r.rid == s["rid"] and list(r.blast.nb) == s["nb"] and np.dtype(r.dtype).name == s["dtype"]
+        for a, b in ((r.arrival, s["arrival"]), (r.blast.radius, s["radius"]), (r.blast.p_in, s["p_in"]),
+                     (r.blast.t_end, s["t_end"])):
+            assert abs(a - b) <= 1e-8 * max(1.0, abs(b))
+        assert all(abs(a - b) <= 1e-8 * max(1.0, abs(b)) for a, b in zip(r.blast.centre, s["centre"]))
+    slow = request_stream(10.0, seed=saved["seed"], count=saved["count"])
+    for a, b in zip(slow, reqs):
+        assert a.blast.nb == b.blast.nb and abs(a.arrival - 10.0 * b.arrival) <= 1e-9 * max(1.0, a.arrival)
