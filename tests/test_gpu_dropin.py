@@ -10,6 +10,7 @@ import re
 import subprocess
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
@@ -72,3 +73,29 @@ def test_dropin_main_matches_reference_program(prog, args, env, tmp_path):
     assert files and files == sorted(p.name for p in (tmp_path / "gpu").glob("*.csv"))
     for f in files:
         assert (tmp_path / "gpu" / f).read_bytes() == (tmp_path / "cpu" / f).read_bytes(), f
+
+
+@pytest.mark.parametrize("prog,args", [CASES[0], ("hydro3d", ["-x", "20", "-y", "16", "-z", "12", "-t", "2",
+                                                              "-i", "60", "-w", "60"])])
+def test_dropin_fused_arithmetic(prog, args, tmp_path):
+    """The unchanged host program in the fused arithmetic (HYDRO_B200_ARITH=fused): the
+    printed t, Dt and mass lines equal the reference program's at their printed precision,
+    and every CSV value is within 2e-5 relative (6 printed digits) of the reference's, or
+    within 1e-13 of its column's largest magnitude (momenta near zero ahead of the wave
+    differ from strict by a few ulp of the momenta's scale)."""
+    gpu, cpu = REFDIR / f"{prog}.cuda", REFDIR / f"{prog}.cpu"
+    if not gpu.exists() or not cpu.exists():
+        pytest.skip("oracle/_ref drop-in binaries not built")
+    (tmp_path / "gpu").mkdir()
+    (tmp_path / "cpu").mkdir()
+    out_gpu = run(gpu, args, tmp_path / "gpu", True, {"HYDRO_B200_ARITH": "fused"})
+    out_cpu = run(cpu, args, tmp_path / "cpu", True)
+    assert out_gpu == out_cpu
+    files = sorted(p.name for p in (tmp_path / "cpu").glob("*.csv"))
+    assert files and files == sorted(p.name for p in (tmp_path / "gpu").glob("*.csv"))
+    for f in files:
+        a = np.loadtxt(tmp_path / "gpu" / f, delimiter=",", skiprows=1)
+        b = np.loadtxt(tmp_path / "cpu" / f, delimiter=",", skiprows=1)
+        assert a.shape == b.shape
+        scale = np.abs(b).max(axis=0, keepdims=True)
+        assert np.all(np.abs(a - b) <= 2e-5 * np.abs(b) + 1e-13 * scale), f
