@@ -743,9 +743,10 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="iterations of the FP32-vs-FP64 accuracy runs on the large grids")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serving-rates", type=float, nargs="+", default=[10.0, 100.0, 1000.0])
-    ap.add_argument("--serving-requests", type=int, default=8)
-    ap.add_argument("--serving-wall", type=float, default=20.0, help="cap per serving run, seconds")
+    ap.add_argument("--serving-rates", type=float, nargs="+", default=[1000.0],
+                    help="request rates (the default run: one rate; --serving-sweep: pass 10 30 100 300 1000)")
+    ap.add_argument("--serving-requests", type=int, default=16)
+    ap.add_argument("--serving-wall", type=float, default=40.0, help="cap per serving run, seconds")
     ap.add_argument("--no-serving-plain", action="store_true")
     ap.add_argument("--serving-sweep", action="store_true",
                     help="the serving workload as configured (rates 10..1000/s, 200 requests each, plus a "
