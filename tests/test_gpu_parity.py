@@ -73,6 +73,9 @@ def test_step3d_bitwise(cuda, oracle, nb, T, kernel):
         dref = oracle.step(st, ref, phys, dtd)
         out, d, info = gpu_step(cuda, st, phys, dtd, kernel)
         assert info.kernel == kernel
+        if kernel == hb.KERNEL_STRIP:
+            # FP64 planes by tensor maps where the rows are 16-byte pitched (even NB_Z)
+            assert hb.last_launch_shape()["tma"] == (T is np.float64 and nb[2] % 2 == 0)
         assert d.tobytes() == dref.tobytes()
         assert out[0].tobytes() == ref[0].tobytes()
         assert out[1].tobytes() == ref[1].tobytes()
