@@ -14,6 +14,7 @@ from __future__ import annotations
 import ctypes
 import os
 import subprocess
+import sys
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -66,7 +67,13 @@ def build(force: bool = False) -> None:
     nvcc = Path(os.environ.get("CUDA", "/usr/local/cuda")) / "bin" / "nvcc"
     if not nvcc.exists() and LIB_PATH.exists() and not force:
         return
-    subprocess.run(["make", "-C", str(PKG_DIR), "-j8"] + (["-B"] if force else []), check=True)
+    # make's report goes to stderr: stdout belongs to the caller (bench.py prints one JSON line)
+    p = subprocess.run(["make", "-C", str(PKG_DIR), "-j8", "--no-print-directory"] + (["-B"] if force else []),
+                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if p.stdout and "Nothing to be done" not in p.stdout:
+        sys.stderr.write(p.stdout)
+    if p.returncode != 0:
+        raise HydroError(-1, f"building the CUDA library failed (make exit {p.returncode})")
 
 
 _lib = None
