@@ -15,8 +15,10 @@ Batched path (`tune`): the batched kernels take a fixed block shape (2D: 128 lan
 126 interior columns; 3D: 8 x 32 lanes over 6 x 30 interior columns in FP64, 16 x 32 over
 14 x 30 in FP32) and one free tile parameter, the rows (planes) a work item marches,
 `chunk`. Longer chunks re-read fewer halo rows and take fewer work items; shorter ones
-balance uneven instances better. `tune` times a seeded mini-batch of the batched
-workload for each candidate and keeps the fastest.
+balance uneven instances better, so the best value depends on how much work a step holds:
+`tune` times a batch drawn like the batched workload in 2D (256 seeded blasts, sides
+log-uniform in [64, 2048]; a smaller batch favours shorter chunks) and 48 seeded 3D blasts
+with sides in [32, 256] in 3D, for each candidate, and keeps the fastest.
 
 Results are cached per (GPU name, dimensionality, precision[, arithmetic]) in a JSON file
 next to this module (written on the machine that runs it, not shipped).
@@ -35,7 +37,8 @@ from .batch import Batch
 from .workloads import batch_blasts
 
 CACHE = Path(os.environ.get("HYDRO_B200_TUNE_CACHE", Path(__file__).resolve().parent / "autotune_cache.json"))
-CANDIDATES = {2: (32, 64, 128, 256, 512), 3: (16, 32, 64, 128)}
+CANDIDATES = {2: (32, 48, 64, 96, 128, 256), 3: (16, 32, 64, 128)}
+TUNE_INSTANCES = {2: 256, 3: 48}
 
 
 def _key(dim, dtype):
@@ -60,7 +63,7 @@ def _blasts(dim, n, seed):
 
 
 def measure(dim, dtype, chunk, n=48, steps=6, seed=11):
-    """Cell-updates per second of the batched step on a seeded mini-batch."""
+    """Cell-updates per second of the batched step on `n` seeded blasts."""
     torch = _torch()
     blasts = _blasts(dim, n, seed)
     s = torch.cuda.Stream()
@@ -82,12 +85,13 @@ def measure(dim, dtype, chunk, n=48, steps=6, seed=11):
     return cells * steps / (ms / 1e3)
 
 
-def tune(dim, dtype, force=False, log=None, candidates=None, n=48, steps=6):
+def tune(dim, dtype, force=False, log=None, candidates=None, n=None, steps=10):
     """The fastest chunk for (this GPU, dim, dtype), measured once and then cached."""
     cache = _load()
     key = _key(dim, dtype)
     if key in cache and not force:
         return int(cache[key]["chunk"])
+    n = n or TUNE_INSTANCES[dim]
     results = {}
     for c in candidates or CANDIDATES[dim]:
         t0 = time.perf_counter()

@@ -89,6 +89,10 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
     // their primitives are never used, so they convert a unit state instead (keeps the
     // reciprocal / square root of every lane on its regular path)
     const bool real_col = (j >= 1) && (j <= g.nb_y);
+    // a warp whose first column is past the last ghost column (NB_Y+1) computes nothing
+    // that is used: no interior cell, and its lane 0's cell only enters the face
+    // (NB_Y+1 | NB_Y+2) of the warp before it. It takes part in the row barriers only.
+    const bool dead_warp = kEdge && (g.jbase + (t & ~31) > g.nb_y + 1);
     const unsigned ld0 = ld;
 
     auto issue = [&](int m) {
@@ -126,6 +130,11 @@ __device__ __forceinline__ bool march2d_strip(Smem2<T> &S, const CUtensorMap *tm
     for (; m < nrows; ++m) {
         const unsigned q = ld0 + (unsigned)m;
         const int s = q % kStages;
+        if (kEdge && dead_warp) {
+            __syncthreads();
+            if (S.abort) break;
+            continue; // (thread 0, which issues the row loads, is in warp 0: never dead)
+        }
         if constexpr (kTma) {
             if (!mbar_wait_bounded(&S.full[s], (q / kStages) & 1)) S.abort = 1;
         } else {
