@@ -12,9 +12,8 @@ candidate, keeps the fastest and installs it in the library (hydro_set_launch_sh
 results do not depend on the shape.
 
 Batched path (`tune`): the batched kernels take a fixed block shape (2D: 128 lanes over
-126 interior columns; 3D: 8 x 32 lanes over 6 x 30 interior columns in FP64, 16 x 32 over
-14 x 30 in FP32) and one free tile parameter, the rows (planes) a work item marches,
-`chunk`. Longer chunks re-read fewer halo rows and take fewer work items; shorter ones
+126 interior columns; 3D: 8 x 32 lanes over 6 x 30 interior columns) and one free tile
+parameter, the rows (planes) a work item marches, `chunk`. Longer chunks re-read fewer halo rows and take fewer work items; shorter ones
 balance uneven instances better, so the best value depends on how much work a step holds:
 `tune` times a batch drawn like the batched workload in 2D (256 seeded blasts, sides
 log-uniform in [64, 2048]; a smaller batch favours shorter chunks) and 48 seeded 3D blasts

@@ -110,7 +110,7 @@ template <class T, bool kF = false> __global__ void __launch_bounds__(k3RedoNT) 
 // kF: fused arithmetic (hydro_math.cuh). kTma: planes staged by the tensor maps tmr/tmu
 // (FP64, even NB_Z), else by per-lane cp.async. W: warps per block (tile rows with halo).
 template <class T, bool kF, bool kTma, int W>
-__global__ void __launch_bounds__(32 * W, min_blocks3(W))
+__global__ void __launch_bounds__(32 * W, min_blocks3<T>(W))
     strip3d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args3<T> g)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(32 * W, min_blocks3(W))
 }
 
 // Tile heights the plain 3D step is built for: FP64 8 (default), 12 and 16 warps; FP32 8
-// and 16 (default). The tensor-map staging is built for FP64 only.
+// (default) and 16. The tensor-map staging is built for FP64 only.
 template <class T> constexpr bool tile3_built(int W)
 {
     return sizeof(T) == 8 ? (W == 8 || W == 12 || W == 16) : (W == 8 || W == 16);
@@ -296,7 +296,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         // planes per block: sized for about 8 waves of resident blocks, at least 8 and at
         // most the cap (the tuned value when one is set, else 256)
         const int cap = shape.chunk > 0 ? shape.chunk : 256;
-        const int target = device_sms() * min_blocks3(W) * 8;
+        const int target = device_sms() * min_blocks3<T>(W) * 8;
         int nchunks = std::max(1, (target + nz * ny - 1) / (nz * ny));
         int chunk = (int)((nb_x + nchunks - 1) / nchunks);
         chunk = std::min(cap, std::max(std::min(8, cap), chunk));
@@ -342,7 +342,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         }
         ctx->last_warps = W;
         ctx->last_chunk = chunk;
-        ctx->last_blocks = min_blocks3(W);
+        ctx->last_blocks = min_blocks3<T>(W);
         ctx->last_tma = tma;
     } else {
         const int gx = (int)((nb_z + 31) / 32), gy = (int)((nb_y + 3) / 4), gz = (int)std::min<size_t>(nb_x, 65535);

@@ -2,7 +2,7 @@
 // chunk per block) and the batched step (batch3d, tiles of many instances per persistent
 // block).
 //
-// One block of 8 (FP64) or 16 (FP32) warps covers a (warps) y x 32 z tile of columns
+// One block of W warps (8 by default) covers a W y x 32 z tile of columns
 // starting at (jbase, kbase): the interior columns plus a one-cell halo ring. Each X plane
 // of the tile arrives in a k3Stages-deep shared-memory ring, in one of two forms:
 //  - tensor maps (kTma): one thread issues two 3D TMA tile loads per plane (the (rho, E)
@@ -23,17 +23,17 @@
 
 namespace hydro {
 
-// Tile height per precision: FP32 keeps 16 warps (14 interior rows; one 512-thread block
-// per SM), FP64 8 warps (6 interior rows; two 256-thread blocks per SM, the most its
-// 128-register budget allows). Measured at 512^3: FP32 48.3 -> 50.1 GCell/s with 16 warps,
-// FP64 31.5 -> 28.4 (it spills and loses the second block).
+// Tile height: 8 warps (6 interior rows) in both precisions. Resident blocks per SM of an
+// 8-warp tile: FP64 two (the 128-register budget; with 16 warps it spills and keeps one
+// block, 31.5 -> 28.4 GCell/s at 512^3), FP32 three (80 registers without spills; 54.1 ->
+// 56.2 GCell/s at 512^3 against two, and 16-warp tiles with one block give 53.7).
 // The plain step also takes other tile heights (warps W per block, W - 2 interior rows),
 // chosen at run time (hydro_set_launch_shape): k3Warps is the default.
-template <class T> constexpr int k3Warps = sizeof(T) == 4 ? 16 : 8; // y extent of the tile (with halo)
+template <class T> constexpr int min_blocks3(int W) { return W <= 8 ? (sizeof(T) == 4 ? 3 : 2) : 1; }
+template <class T> constexpr int k3Warps = 8;                        // y extent of the tile (with halo)
 template <class T> constexpr int k3NT = 32 * k3Warps<T>;             // threads
 template <class T> constexpr int k3TY = k3Warps<T> - 2;              // interior rows per tile
-template <class T> constexpr int k3MinBlocks = k3Warps<T> <= 8 ? 2 : 1; // resident blocks per SM
-constexpr int min_blocks3(int W) { return W <= 8 ? 2 : 1; }
+template <class T> constexpr int k3MinBlocks = min_blocks3<T>(k3Warps<T>); // resident blocks per SM
 constexpr int k3TZ = 30;           // interior columns per tile
 constexpr int k3Stages = 4;
 

@@ -60,7 +60,7 @@ def test_step2d_bitwise(cuda, oracle, nb, T, kernel):
 
 @pytest.mark.parametrize("kernel", [hb.KERNEL_STRIP, hb.KERNEL_DIRECT])
 @pytest.mark.parametrize("T", [np.float64, np.float32])
-# (40, 150, 130): 25 x 5 tiles per plane in FP64 (11 x 5 in FP32), most of them interior
+# (40, 150, 130): 25 x 5 tiles per plane (8-warp tiles), most of them interior
 # tiles that take the lean march
 @pytest.mark.parametrize("nb", SHAPES_3D + [(9, 14, 61), (4, 7, 30), (6, 13, 31), (5, 6, 62), (40, 150, 130)])
 def test_step3d_bitwise(cuda, oracle, nb, T, kernel):
