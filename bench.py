@@ -866,6 +866,8 @@ def main():
     achieved = cells * bpc / (kern_ms / 1e3) / 1e9
     roofline = dict(bound="hbm", achieved=achieved, peak=hbm, unit="GB/s", frac=achieved / hbm,
                     peak_kind=peak_kind, traffic=None, kernel=kname, bytes_per_cell=bpc, kernel_ms=kern_ms,
+                    kernel_ms_median=statistics.median(r["kernel_ms"]), kernel_ms_min=min(r["kernel_ms"]),
+                    kernel_ms_max=max(r["kernel_ms"]), frac_of_nominal_8tbs=achieved / 8000.0,
                     arith=args.arith, launch_shape=r["shape"])
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
@@ -909,6 +911,8 @@ def main():
             variants[name] = dict(value=world * vc * nst / (vms / 1e3) / 1e9, unit=UNIT,
                                   kernel_gbs=vc * vbpc / (km / 1e3) / 1e9, frac=vc * vbpc / (km / 1e3) / 1e9 / hbm,
                                   kernel=int(vr["kernel"]), ms_per_step=vms / nst, clocks=vclocks,
+                                  kernel_ms_median=statistics.median(vr["kernel_ms"]),
+                                  kernel_ms_spread=max(vr["kernel_ms"]) - min(vr["kernel_ms"]),
                                   launch_shape=vr["shape"])
 
     accuracy = {}
