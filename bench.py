@@ -85,6 +85,11 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
+            # wait (at most 2 s) for its first sample, so that nvidia-smi's start-up does not
+            # compete with the host loop of the timed region
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 2.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
@@ -900,11 +905,11 @@ def main():
             barrier()
             vsampler = ClockSampler(uuid)
             vsampler.start()
-            vr = bench_resident(hb, torch, vnb, T, max(5, args.steps // 3), 3, arith=ar)
+            vr = bench_resident(hb, torch, vnb, T, max(10, args.steps // 2), 3, arith=ar)
             vclocks = vsampler.stop()
             barrier()
             vms = max_over_ranks(vr["total_ms"])
-            nst = max(5, args.steps // 3)
+            nst = max(10, args.steps // 2)
             vc = int(np.prod(vnb))
             km = statistics.mean(vr["kernel_ms"])
             vbpc = BYTES_PER_CELL[(len(vnb), np.dtype(T).itemsize)]
