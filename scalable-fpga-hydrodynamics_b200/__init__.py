@@ -67,9 +67,15 @@ def build(force: bool = False) -> None:
     nvcc = Path(os.environ.get("CUDA", "/usr/local/cuda")) / "bin" / "nvcc"
     if not nvcc.exists() and LIB_PATH.exists() and not force:
         return
-    # make's report goes to stderr: stdout belongs to the caller (bench.py prints one JSON line)
-    p = subprocess.run(["make", "-C", str(PKG_DIR), "-j8", "--no-print-directory"] + (["-B"] if force else []),
-                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    # one make at a time (ranks of one job build the same tree); make's report goes to
+    # stderr: stdout belongs to the caller (bench.py prints one JSON line)
+    import fcntl
+
+    LIB_DIR.mkdir(exist_ok=True)
+    with open(LIB_DIR / ".build.lock", "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        p = subprocess.run(["make", "-C", str(PKG_DIR), "-j8", "--no-print-directory"] + (["-B"] if force else []),
+                           stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     if p.stdout and "Nothing to be done" not in p.stdout:
         sys.stderr.write(p.stdout)
     if p.returncode != 0:
