@@ -95,3 +95,40 @@ def test_launch_shape_settings(built):
         for pb in (4, 8):
             assert fn(dim, pb, 0, 0, 0) == 0
     built.hydro_clear_error()
+
+
+def test_step_arguments_rejected_before_any_device_call(built):
+    """The step entry points reject null pointers and grids past their limits (NB > 2^30 per
+    axis, more than 2^40 cells in 2D / 1e12 in 3D) with HYDRO_ERR_ARG and a message, before
+    any CUDA call: the pointers below are never dereferenced."""
+    fake = ctypes.c_void_p(256)
+    d, f, sz = ctypes.c_double, ctypes.c_float, ctypes.c_size_t
+    for suf, T in (("f64", d), ("f32", f)):
+        fn2 = getattr(built, f"hydro2d_step_{suf}")
+        fn2.argtypes = [ctypes.c_void_p] * 5 + [T] * 5 + [sz] * 2 + [T] * 2 + [ctypes.c_void_p, ctypes.c_int,
+                                                                             ctypes.c_int, ctypes.c_void_p]
+        fn2.restype = ctypes.c_int
+        fn3 = getattr(built, f"hydro3d_step_{suf}")
+        fn3.argtypes = [ctypes.c_void_p] * 5 + [T] * 5 + [sz] * 3 + [T] * 3 + [ctypes.c_void_p, ctypes.c_int,
+                                                                              ctypes.c_int, ctypes.c_void_p]
+        fn3.restype = ctypes.c_int
+        phys = (0.1, 1.4, 0.4, 1 / 0.4, 1.1)
+        cases2 = [((None, fake, fake, fake, fake), (16, 16), "null pointer"),
+                  ((fake,) * 5, ((1 << 30) + 1, 4), "too large"),
+                  ((fake,) * 5, (4, (1 << 30) + 1), "too large"),
+                  ((fake,) * 5, ((1 << 21), (1 << 20)), "too large")]
+        for ptrs, nb, msg in cases2:
+            built.hydro_clear_error()
+            assert fn2(*ptrs, *phys, *nb, 1e-3, 1e-3, None, 0, 1, None) == hb.HYDRO_ERR_ARG, (suf, nb)
+            code, text = hb.last_error()
+            assert code == hb.HYDRO_ERR_ARG and msg in text, text
+        cases3 = [((fake, fake, None, fake, fake), (8, 8, 8), "null pointer"),
+                  ((fake,) * 5, ((1 << 30) + 1, 2, 2), "too large"),
+                  ((fake,) * 5, (2, 2, (1 << 30) + 1), "too large"),
+                  ((fake,) * 5, (10000, 10000, 10001), "too large")]
+        for ptrs, nb, msg in cases3:
+            built.hydro_clear_error()
+            assert fn3(*ptrs, *phys, *nb, 1e-3, 1e-3, 1e-3, None, 0, 1, None) == hb.HYDRO_ERR_ARG, (suf, nb)
+            code, text = hb.last_error()
+            assert code == hb.HYDRO_ERR_ARG and msg in text, text
+    built.hydro_clear_error()
