@@ -52,10 +52,25 @@ SLAB_CASES = [
     ("hydro_float", ["-x", "60", "-y", "60", "-t", "2", "-i", "120", "-w", "40", "--sdx", "2", "--sdy", "1"]),
     ("hydro3d", ["-x", "20", "-y", "16", "-z", "12", "-t", "2", "-i", "40", "-w", "20", "--sdx", "2", "--sdy", "1"]),
 ]
+# Y (and 3D Z) splits (--sdy N, --sdz N): the reference kernel mirrors the walls at every
+# subdomain's own edges (hydro2d/kernel.cxx:225-247, the is_top_wall / is_bottom_wall
+# selects; hydro3d/kernel.cxx:238-320), whatever the host
+# exchanged into its Y ghost columns, as the kernels here do; with one X subdomain the X
+# neighbours wrap in-kernel, with several they come from the X ghost rows
+YSPLIT_CASES = [
+    (("hydro", ["-x", "60", "-y", "60", "-t", "2", "-i", "80", "-w", "40", "--sdx", "1", "--sdy", "2"]), None),
+    (("hydro", ["-x", "48", "-y", "50", "-t", "2", "-i", "60", "-w", "30", "--sdx", "2", "--sdy", "3"]),
+     {"HYDRO_B200_X_GHOSTS": "memory"}),
+    (("hydro3d", ["-x", "12", "-y", "20", "-z", "10", "-t", "2", "-i", "30", "-w", "15", "--sdx", "1", "--sdy", "2"]),
+     None),
+    (("hydro3d", ["-x", "12", "-y", "10", "-z", "20", "-t", "2", "-i", "30", "-w", "15", "--sdx", "2", "--sdy", "1",
+                  "--sdz", "2"]), {"HYDRO_B200_X_GHOSTS": "memory"}),
+]
 
 
 @pytest.mark.parametrize("prog,args,env", [(p, a, None) for p, a in CASES] +
-                         [(p, a, {"HYDRO_B200_X_GHOSTS": "memory"}) for p, a in SLAB_CASES])
+                         [(p, a, {"HYDRO_B200_X_GHOSTS": "memory"}) for p, a in SLAB_CASES] +
+                         [(p, a, e) for (p, a), e in YSPLIT_CASES])
 def test_dropin_main_matches_reference_program(prog, args, env, tmp_path):
     gpu, cpu = REFDIR / f"{prog}.cuda", REFDIR / f"{prog}.cpu"
     if not gpu.exists() or not cpu.exists():
