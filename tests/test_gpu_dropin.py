@@ -53,8 +53,8 @@ SLAB_CASES = [
     ("hydro3d", ["-x", "20", "-y", "16", "-z", "12", "-t", "2", "-i", "40", "-w", "20", "--sdx", "2", "--sdy", "1"]),
 ]
 # Y (and 3D Z) splits (--sdy N, --sdz N): the reference kernel mirrors the walls at every
-# subdomain's own edges (hydro2d/kernel.cxx:225-247, the is_top_wall / is_bottom_wall
-# selects; hydro3d/kernel.cxx:238-320), whatever the host
+# subdomain's own edges (hydro2d/kernel.cxx:214-245, the is_top_wall / is_bottom_wall
+# selects; hydro3d/kernel.cxx:240-320), whatever the host
 # exchanged into its Y ghost columns, as the kernels here do; with one X subdomain the X
 # neighbours wrap in-kernel, with several they come from the X ghost rows
 YSPLIT_CASES = [
