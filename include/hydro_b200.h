@@ -196,8 +196,11 @@ unsigned hydro2d_noalloc_launch_shape(size_t NB_X, size_t NB_Y, int strip, int s
 
 /* Launch shape of the plain strip kernels for (dim 2 or 3, precision 4 or 8 bytes), as an
  * autotuner picks it. 0 keeps the built-in choice for any field.
- *  warps: 3D only, warps per block, i.e. tile rows with the one-row halo (8, 16, and 12 in
- *    FP64; built-in 8 in FP64, 16 in FP32);
+ *  warps: 3D only, the tile height in rows with the one-row halo (8, 16, and in FP64 also
+ *    9 and 12). Tiles of 8, 12 and 16 rows run one warp per row; a 9-row tile runs on 8
+ *    warps, warp 0 holding both halo rows, and needs the tensor-map staging (FP64 with an
+ *    even NB_Z and 16-byte aligned arrays; elsewhere 8 rows run). Built-in: 9 where the
+ *    tensor maps apply, else 8;
  *  chunk: the most rows (2D) or planes (3D) one block marches (built-in 256); blocks take
  *    fewer on grids too small to fill the GPU with that many (sized from the grid and the
  *    SM count);
@@ -206,7 +209,8 @@ unsigned hydro2d_noalloc_launch_shape(size_t NB_X, size_t NB_Y, int strip, int s
  * Process-wide; the results do not depend on the shape. No counterpart in the reference,
  * whose single-task kernel has no launch shape. */
 int hydro_set_launch_shape(int dim, int precision_bytes, int warps, int chunk, int blocks_per_sm);
-/* The shape the last strip-kernel step on the current device used (warps 0 in 2D), and
+/* The shape the last strip-kernel step on the current device used (warps: the 3D tile
+ * height in rows as above, 0 in 2D), and
  * whether its rows / planes were staged by tensor-map loads (1) or per-lane copies (0). */
 int hydro_last_launch_shape(int *warps, int *chunk, int *blocks_per_sm, int *tma);
 

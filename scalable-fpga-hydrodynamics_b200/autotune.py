@@ -3,9 +3,11 @@
 Plain path (`tune_plain`): the strip kernels take two shape parameters each. Both take the
 most X rows (2D) or planes (3D) one block marches (`chunk`, 0 for the built-in 256; grids
 too small to fill the GPU with such blocks take fewer, so a value tuned on one grid suits
-others): longer chunks re-read fewer halo rows but give fewer blocks. The 3D kernel also takes its tile height (warps per block, i.e. tile rows with the
-one-row halo: 8, 12 or 16 in FP64, 8 or 16 in FP32): taller tiles recompute fewer halo
-rows but hold one block per SM. The 2D kernel also takes its register budget in resident
+others): longer chunks re-read fewer halo rows but give fewer blocks. The 3D kernel also
+takes its tile height in rows with the one-row halo: 8, 9, 12 or 16 in FP64, 8 or 16 in
+FP32. Tiles of 8, 12 and 16 rows run one warp per row (taller tiles recompute fewer halo
+rows but hold one block per SM); the 9-row tile runs on 8 warps, warp 0 holding both halo
+rows (FP64 with tensor-map staging). The 2D kernel also takes its register budget in resident
 blocks per SM (4, or 5 in FP64 / 8 in FP32): more resident warps against fewer registers
 per thread. `tune_plain` times a few steps of the blast on the grid it is given for every
 candidate, keeps the fastest and installs it in the library (hydro_set_launch_shape); the
@@ -112,10 +114,10 @@ def best_chunk(dim, dtype):
     return int(entry["chunk"]) if entry else 0
 
 
-# plain-path candidates per (dim, precision bytes): (3D warps per block or 2D blocks per
-# SM, the other 0) and chunks
+# plain-path candidates per (dim, precision bytes): (3D tile rows with halo or 2D blocks
+# per SM, the other 0) and chunks
 PLAIN_SHAPES = {(2, 4): [(0, 4), (0, 8)], (2, 8): [(0, 4), (0, 5)], (3, 4): [(8, 0), (16, 0)],
-                (3, 8): [(8, 0), (12, 0), (16, 0)]}
+                (3, 8): [(9, 0), (8, 0), (12, 0), (16, 0)]}
 PLAIN_CHUNKS = {2: (0, 32, 64, 128, 256), 3: (0, 16, 32, 64, 128)}
 
 

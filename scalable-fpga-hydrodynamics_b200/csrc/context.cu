@@ -111,7 +111,8 @@ int set_launch_shape(int dim, size_t tsize, int warps, int chunk, int blocks)
     const int alt_blocks = tsize == 8 ? 5 : 8;
     if ((dim != 2 && dim != 3) || (tsize != 4 && tsize != 8) || chunk < 0 || chunk > (1 << 20) ||
         (dim == 2 && (warps != 0 || (blocks != 0 && blocks != 4 && blocks != alt_blocks))) ||
-        (dim == 3 && (blocks != 0 || (warps != 0 && warps != 8 && warps != 16 && !(tsize == 8 && warps == 12))))) {
+        (dim == 3 && (blocks != 0 || (warps != 0 && warps != 8 && warps != 16 &&
+                                          !(tsize == 8 && (warps == 9 || warps == 12)))))) {
         set_error(kErrArg,
                   "hydro_set_launch_shape: unsupported shape (dim %d, %zu-byte values, %d warps, chunk %d, %d blocks)",
                   dim, tsize, warps, chunk, blocks);

@@ -18,6 +18,7 @@
 //  direct3d  one thread per cell, the 7-point stencil loaded directly, every face
 //            evaluated from both sides like the reference.
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 #include <stdio.h>
 
@@ -108,13 +109,17 @@ template <class T, bool kF = false> __global__ void __launch_bounds__(k3RedoNT) 
 
 // ------------------------------------------------------------------- strip kernel ---
 // kF: fused arithmetic (hydro_math.cuh). kTma: planes staged by the tensor maps tmr/tmu
-// (FP64, even NB_Z), else by per-lane cp.async. W: warps per block (tile rows with halo).
-template <class T, bool kF, bool kTma, int W>
+// (FP64, even NB_Z), else by per-lane cp.async. W: warps per block. Tile rows with halo:
+// W, or W + 1 with kPair (tensor maps, W = 8: warp 0 holds both halo rows).
+template <class T, bool kF, bool kTma, int W, bool kPair = false>
 __global__ void __launch_bounds__(32 * W, min_blocks3<T>(W))
     strip3d(const __grid_constant__ CUtensorMap tmr, const __grid_constant__ CUtensorMap tmu, Args3<T> g)
 {
+    static_assert(!kPair || (kTma && W == 8), "the W+1-row tile is built for tensor maps and 8 warps");
+    using SM = std::conditional_t<kPair, Smem3P<T>, Smem3<T, W>>;
+    constexpr int kRows = kPair ? W + 1 : W;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    Smem3<T, W> &S = *reinterpret_cast<Smem3<T, W> *>(smem_raw);
+    SM &S = *reinterpret_cast<SM *>(smem_raw);
     if constexpr (kTma) {
         if (threadIdx.x == 0) {
             prefetch_tensormap(&tmr);
@@ -123,44 +128,57 @@ __global__ void __launch_bounds__(32 * W, min_blocks3<T>(W))
         march3d_init(S);
     }
     const int i0 = 1 + g.chunk * (int)blockIdx.z;
-    const March3 geo{k3TZ * (int)blockIdx.x, (W - 2) * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
+    const March3 geo{k3TZ * (int)blockIdx.x, (kRows - 2) * (int)blockIdx.y, i0, min(i0 + g.chunk - 1, g.nb_x),
                      g.nb_x, g.nb_y, g.nb_z, g.zs, g.zy, g.xwrap};
     StepAcc acc;
     const float tlof = __double2float_rd(skip_threshold(g.scr, g.key));
     const float tlo2 = skip_tlo2(tlof), ggm1 = g.ggm1;
     const Phys<T> ph = g.ph;
-    const bool ok = march3d<T, kF, kTma, W>(
-        S, g.rhoE, g.uvw, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz,
-        [&](const Upd3<T> &o) {
-            acc.add_mass(o.r);
-            if (!state_below(o, ggm1, tlo2))
-                acc.add_speed(speed3<T, kF>(o.r, o.u, o.v, o.w, o.E, ph));
-        },
-        Tmaps3{&tmr, &tmu});
+    auto sink = [&](const Upd3<T> &o) {
+        acc.add_mass(o.r);
+        if (!state_below(o, ggm1, tlo2))
+            acc.add_speed(speed3<T, kF>(o.r, o.u, o.v, o.w, o.E, ph));
+    };
+    bool ok;
+    if constexpr (kPair)
+        ok = march3d<T, kF>(S, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz, sink, Tmaps3{&tmr, &tmu});
+    else
+        ok = march3d<T, kF, kTma, W>(S, g.rhoE, g.uvw, g.rhoE_n, g.uvw_n, geo, ph, g.DtDx, g.DtDy, g.DtDz, sink,
+                                     Tmaps3{&tmr, &tmu});
     if (!ok) acc.err |= kErrWaitTimeout;
     step_epilogue<32 * W, T>(acc, g.scr, g.partials, gridDim.x * gridDim.y * gridDim.z,
                              blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z), g.ph.C_min, g.Dt_next,
                              g.status, g.seq, (double)tlof, g.key);
 }
 
-// Tile heights the plain 3D step is built for: FP64 8 (default), 12 and 16 warps; FP32 8
-// (default) and 16. The tensor-map staging is built for FP64 only.
-template <class T> constexpr bool tile3_built(int W)
+// Tile heights (rows with halo) the plain 3D step is built for: FP64 8, 9 (8 warps, warp 0
+// holding both halo rows; tensor-map staging only), 12 and 16; FP32 8 and 16. The
+// tensor-map staging is built for FP64 only.
+template <class T> constexpr bool tile3_built(int rows)
 {
-    return sizeof(T) == 8 ? (W == 8 || W == 12 || W == 16) : (W == 8 || W == 16);
+    return sizeof(T) == 8 ? (rows == 8 || rows == 9 || rows == 12 || rows == 16) : (rows == 8 || rows == 16);
 }
+// The built-in tile height: 9 rows where tensor maps stage the planes (FP64: 37.2 against
+// 35.3 GCell/s strict at 512^3 for 8 rows), else 8.
+template <class T> int default_rows3(bool tma) { return (sizeof(T) == 8 && tma) ? 9 : k3Warps<T>; }
 
-template <class T, int W>
+template <class T, int W, bool kPair = false>
 cudaError_t launch_strip3d(bool fused, bool tma, dim3 grid, cudaStream_t stream, const CUtensorMap &tmr,
                            const CUtensorMap &tmu, const Args3<T> &g)
 {
     void (*kern)(const CUtensorMap, const CUtensorMap, Args3<T>);
-    if constexpr (sizeof(T) == 8)
-        kern = fused ? (tma ? strip3d<T, true, true, W> : strip3d<T, true, false, W>)
-                     : (tma ? strip3d<T, false, true, W> : strip3d<T, false, false, W>);
-    else
-        kern = fused ? strip3d<T, true, false, W> : strip3d<T, false, false, W>;
-    const int smem = (int)sizeof(Smem3<T, W>);
+    int smem;
+    if constexpr (kPair) {
+        kern = fused ? strip3d<T, true, true, W, true> : strip3d<T, false, true, W, true>;
+        smem = (int)sizeof(Smem3P<T>);
+    } else {
+        if constexpr (sizeof(T) == 8)
+            kern = fused ? (tma ? strip3d<T, true, true, W> : strip3d<T, true, false, W>)
+                         : (tma ? strip3d<T, false, true, W> : strip3d<T, false, false, W>);
+        else
+            kern = fused ? strip3d<T, true, false, W> : strip3d<T, false, false, W>;
+        smem = (int)sizeof(Smem3<T, W>);
+    }
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     kern<<<grid, 32 * W, smem, stream>>>(tmr, tmu, g);
@@ -287,8 +305,15 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         // tile height and planes per block: the tuned shape when one is set
         // (hydro_set_launch_shape), else the built-in one
         const LaunchShape shape = launch_shape(3, sizeof(T));
-        const int W = (shape.warps > 0 && tile3_built<T>(shape.warps)) ? shape.warps : k3Warps<T>;
-        const int nz = (int)((nb_z + k3TZ - 1) / k3TZ), ny = (int)((nb_y + (W - 2) - 1) / (W - 2));
+        // planes by tensor maps where the rows of both arrays are 16-byte pitched (FP64
+        // with even NB_Z; the tile's kbase is a multiple of 30, so even) and the arrays
+        // 16-byte aligned; by per-lane copies otherwise
+        bool tma = sizeof(T) == 8 && (nb_z + 2) % 2 == 0 && aligned16(rhoE) && aligned16(uvw);
+        // tile rows with halo; the 9-row tile needs the tensor maps (else 8 rows)
+        int rows = (shape.warps > 0 && tile3_built<T>(shape.warps)) ? shape.warps : default_rows3<T>(tma);
+        if (rows == 9 && !tma) rows = 8;
+        const int W = rows == 9 ? 8 : rows; // warps per block
+        const int nz = (int)((nb_z + k3TZ - 1) / k3TZ), ny = (int)((nb_y + (rows - 2) - 1) / (rows - 2));
         if (ny > 65535) {
             set_error(kErrArg, "step3d: NB_Y %zu too large for the strip kernel", nb_y);
             return kErrArg;
@@ -309,23 +334,28 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
         nblocks = (unsigned)nz * ny * nchunks;
         if ((err = ctx_reserve(ctx, nblocks)) != kOk) return err;
         g.partials = ctx->partials;
-        // planes by tensor maps where the rows of both arrays are 16-byte pitched (FP64
-        // with even NB_Z; the tile's kbase is a multiple of 30, so even) and the arrays
-        // 16-byte aligned; by per-lane copies otherwise
         CUtensorMap tmr, tmu;
         std::memset(&tmr, 0, sizeof tmr);
         std::memset(&tmu, 0, sizeof tmu);
-        bool tma = sizeof(T) == 8 && (nb_z + 2) % 2 == 0 && aligned16(rhoE) && aligned16(uvw);
         if (tma) {
             const uint64_t zs = nb_z + 2, ys = nb_y + 2, xs = nb_x + 2;
             tma = encode_tmap_3d(&tmr, tmap_type3<T>(), rhoE, 2 * zs, ys, xs, 2 * zs * sizeof(T), 2 * zs * ys * sizeof(T),
-                                 64, (uint32_t)W, 1) &&
+                                 64, (uint32_t)rows, 1) &&
                   encode_tmap_3d(&tmu, tmap_type3<T>(), uvw, 3 * zs, ys, xs, 3 * zs * sizeof(T), 3 * zs * ys * sizeof(T),
-                                 96, (uint32_t)W, 1);
+                                 96, (uint32_t)rows, 1);
+            if (!tma && rows == 9) {
+                set_error(kErrCuda, "step3d: tensor maps of the 9-row tile rejected");
+                return kErrCuda;
+            }
         }
         const dim3 grid(nz, ny, nchunks);
         cudaError_t ea;
-        if (W == 8) {
+        if (rows == 9) {
+            if constexpr (sizeof(T) == 8)
+                ea = launch_strip3d<T, 8, true>(fused, true, grid, stream, tmr, tmu, g);
+            else
+                ea = cudaErrorInvalidValue;
+        } else if (W == 8) {
             ea = launch_strip3d<T, 8>(fused, tma, grid, stream, tmr, tmu, g);
         } else if constexpr (sizeof(T) == 8) {
             if (W == 12)
@@ -340,7 +370,7 @@ int step3d(const T *rhoE, const T *uvw, T *rhoE_next, T *uvw_next, T *Dt_next, c
             set_error(kErrCuda, "step3d launch: %s", cudaGetErrorString(ea));
             return kErrCuda;
         }
-        ctx->last_warps = W;
+        ctx->last_warps = rows;
         ctx->last_chunk = chunk;
         ctx->last_blocks = min_blocks3<T>(W);
         ctx->last_tma = tma;

@@ -60,8 +60,8 @@ def test_step2d_bitwise(cuda, oracle, nb, T, kernel):
 
 @pytest.mark.parametrize("kernel", [hb.KERNEL_STRIP, hb.KERNEL_DIRECT])
 @pytest.mark.parametrize("T", [np.float64, np.float32])
-# (40, 150, 130): 25 x 5 tiles per plane (8-warp tiles), most of them interior
-# tiles that take the lean march
+# (40, 150, 130): 22 x 5 tiles per plane (9-row FP64 tiles; 25 x 5 with 8 rows), most of
+# them interior tiles that take the lean march
 @pytest.mark.parametrize("nb", SHAPES_3D + [(9, 14, 61), (4, 7, 30), (6, 13, 31), (5, 6, 62), (40, 150, 130)])
 def test_step3d_bitwise(cuda, oracle, nb, T, kernel):
     phys = hb.Physics(T, nb)
@@ -307,9 +307,9 @@ def test_step_x_ghosts_from_memory(cuda, oracle, nb, T, kernel):
 @pytest.mark.parametrize("T", [np.float64, np.float32])
 def test_launch_shapes_bitwise(cuda, oracle, T):
     """Every launch shape the autotuner may pick gives the oracle's bits: 3D tile heights
-    (8, 12, 16 warps in FP64; 8, 16 in FP32) with explicit chunks, 2D register budgets with
-    2D chunks."""
-    warps = (8, 12, 16) if T is np.float64 else (8, 16)
+    (8, 9, 12, 16 rows in FP64; 8, 16 in FP32) with explicit chunks, 2D register budgets
+    with 2D chunks."""
+    warps = (8, 9, 12, 16) if T is np.float64 else (8, 16)
     alt = 5 if T is np.float64 else 8
     cases = [((40, 150, 130), w, c, 0) for w in warps for c in (0, 7, 64)] + \
             [((9, 14, 62), w, 3, 0) for w in warps] + \
