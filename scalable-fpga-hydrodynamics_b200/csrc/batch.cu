@@ -440,12 +440,13 @@ __global__ void __launch_bounds__(k3NT<T>, k3MinBlocks<T>) batch3d(Inst3<T> *ins
         const Phys<T> ph = I->ph;
         MaxAcc acc;
         const float tlo2 = skip_tlo2(batch_threshold(I, skip_frac)), ggm1 = I->ggm1;
-        march3d<T, kF>(S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy,
-                   I->DtDz, [&](const Upd3<T> &o) {
-                       if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
-                       if (!state_below(o, ggm1, tlo2))
-                           acc.add_speed((double)speed3<T, kF>(o.r, o.u, o.v, o.w, o.E, ph));
-                   });
+        march3d<T, kF, false, k3Warps<T>, false>(
+            S, I->rhoE[par], I->uvw[par], I->rhoE[par ^ 1], I->uvw[par ^ 1], geo, ph, I->DtDx, I->DtDy, I->DtDz,
+            [&](const Upd3<T> &o) {
+                if (!(o.r > T(0))) acc.err |= kErrNonPhysical;
+                if (!state_below(o, ggm1, tlo2))
+                    acc.add_speed((double)speed3<T, kF>(o.r, o.u, o.v, o.w, o.E, ph));
+            });
         const int2 rg = ranges[it.x];
         if (publish_step<k3NT<T>>(acc, parts, w, &I->done_items, rg.y, &s_last))
             finalize_step<k3NT<T>, T, kF>(I, parts + rg.x, rg.y, status ? status + it.x : nullptr, skip_frac);

@@ -528,11 +528,196 @@ __device__ __forceinline__ bool march3d_lane(Smem3<T, W> &S, const T *rhoE, cons
     return true;
 }
 
+// Per-lane copies, strict arithmetic: the plane loop written once per warp role, with the
+// interior rows' +y / +z faces of plane m-1, conversion of plane m and x face in one block
+// ahead of the barrier, as in the tensor-map form (512^3 FP32 56.0 -> 57.2 GCell/s; FP64
+// with an odd NB_Z 31.3 -> 34.0). In fused arithmetic this form measured slower (FP32 63.6 ->
+// 60.4, FP64 35.9 -> 30.7 with spills), so fused keeps march3d_lane.
+template <bool kEdge, bool kF, class T, int W, class Sink>
+__device__ __forceinline__ bool march3d_lane_roles(Smem3<T, W> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
+                                               const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &sink)
+{
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int NT = 32 * W;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int k = g.kbase + lane, j = g.jbase + w;
+    const int nplanes = g.i1 - g.i0 + 3;
+    const bool real = !kEdge || ((j >= 1) && (j <= g.nb_y) && (k >= 1) && (k <= g.nb_z));
+    constexpr bool kHaloLoads = sizeof(T) == 4;
+    const bool loader = kHaloLoads ? ((w == 0) || (w == W - 1)) : true;
+    const int rbase = kHaloLoads ? ((w == 0) ? 0 : W / 2) : w;
+    constexpr int kRows = kHaloLoads ? W / 2 : 1;
+    const bool kin = !kEdge || (k <= g.nb_z + 1);
+
+    __syncthreads();
+    auto issue = [&](int m) {
+        const int s = m % k3Stages;
+        if (m < nplanes) {
+            const long long pl =
+                (long long)(g.xwrap ? wrap_plane(g.i0 - 1 + m, g.nb_x) : g.i0 - 1 + m) * g.zy + (long long)g.jbase * g.zs + k;
+#pragma unroll
+            for (int rr = 0; rr < kRows; ++rr) {
+                const int r = rbase + rr;
+                const bool ok = kin && (!kEdge || g.jbase + r <= g.nb_y + 1);
+                const long long c = pl + (long long)r * g.zs;
+                const T *pr = ok ? rhoE + 2 * c : rhoE;
+                const T *pu = ok ? uvw + 3 * c : uvw;
+                const int tt = 32 * r + lane;
+                cp_async(&S.st[s][0][tt], pr, sizeof(T), ok);
+                cp_async(&S.st[s][1][tt], pr + 1, sizeof(T), ok);
+                cp_async(&S.st[s][2][tt], pu, sizeof(T), ok);
+                cp_async(&S.st[s][3][tt], pu + 1, sizeof(T), ok);
+                cp_async(&S.st[s][4][tt], pu + 2, sizeof(T), ok);
+            }
+        }
+        cp_async_commit();
+    };
+    if (loader) {
+#pragma unroll
+        for (int m = 0; m < k3Stages - 1; ++m) issue(m);
+    }
+    if (kHaloLoads) {
+        if (loader) cp_async_wait<k3Stages - 2>();
+        __syncthreads();
+    }
+    // plane m into this lane's registers: the loading lanes refill the stage of plane m-1
+    // and wait for their copies (halo loads: of plane m+1, made visible by this plane's
+    // barrier; own loads: of plane m)
+    auto load = [&](int m, T &ur, T &uE, T &uu, T &uv, T &uw) {
+        const int s = m % k3Stages;
+        if (loader) {
+            issue(m + k3Stages - 1);
+            if (kHaloLoads)
+                cp_async_wait<k3Stages - 2>();
+            else
+                cp_async_wait<k3Stages - 1>();
+        }
+        ur = S.st[s][0][t];
+        uE = S.st[s][1][t];
+        uu = S.st[s][2][t];
+        uv = S.st[s][3][t];
+        uw = S.st[s][4][t];
+        if (kEdge && !real) {
+            ur = T(1);
+            uE = T(1);
+            uu = uv = uw = T(0);
+        }
+    };
+    auto publish = [&](int m, const Cell3<T> &P) {
+        typename Smem3<T, W>::V2 *x = &S.xP[m & 1][0][t];
+        x[0 * NT] = pair3<T>(P.r, P.p);
+        x[1 * NT] = pair3<T>(P.Ka, P.iKa);
+        x[2 * NT] = pair3<T>(P.v, P.w);
+        x[3 * NT] = pair3<T>(P.mu, P.mv);
+        x[4 * NT] = pair3<T>(P.mw, P.eup_xy);
+        if constexpr (!kF) x[5 * NT] = pair3<T>(P.eup_z, T(0));
+    };
+    auto yface = [&](int m, const Cell3<T> &Pme) {
+        const FaceIn3<T> me = face3_y(Pme);
+        const FaceIn3<T> nb = xp_face_y<T, NT>(&S.xP[(m - 1) & 1][0][t + 32]);
+        FaceIn3<T> L = me, R = nb;
+        if (kEdge) {
+            if (j == 0) L = mirror3(nb);
+            if (j == g.nb_y) R = mirror3(me);
+        }
+        return face_flux3<T, kF>(L, R, ph);
+    };
+    auto publish_y = [&](int m, const Flux3<T> &fy) {
+        S.xF[m & 1][0][t] = pair3<T>(fy.r, fy.n);
+        S.xF[m & 1][1][t] = pair3<T>(fy.t1, fy.t2);
+        S.xFE[m & 1][t] = fy.E;
+    };
+    int m = 0;
+    const bool iwarp = (w >= 1) && (w <= (W - 2)) && (!kEdge || (g.jbase + 1 <= g.nb_y));
+    if (iwarp) {
+        const bool interior = (lane >= 1) && (lane <= k3TZ) && (!kEdge || ((j <= g.nb_y) && (k <= g.nb_z)));
+        const long long colofs = (long long)j * g.zs + k;
+        Cell3<T> Pm{};
+        T Ur = 0, Uu = 0, Uv = 0, Uw = 0, UE = 0;
+        Flux3<T> fxlo{};
+        auto zface = [&](int mm) {
+            const FaceIn3<T> mz = face3_z(Pm);
+            const FaceIn3<T> nz = xp_face_z<T, NT, kF>(&S.xP[(mm - 1) & 1][0][t + 1]);
+            FaceIn3<T> L = mz, R = nz;
+            if (kEdge) {
+                if (k == 0) L = mirror3(nz);
+                if (k == g.nb_z) R = mirror3(mz);
+            }
+            return face_flux3<T, kF>(L, R, ph);
+        };
+        for (; m < 2; ++m) {
+            T ur, uE, uu, uv, uw;
+            load(m, ur, uE, uu, uv, uw);
+            const Cell3<T> P = make_cell3<T, kF>(ur, uu, uv, uw, uE, ph);
+            publish(m, P);
+            if (m == 1) fxlo = face_flux3<T, kF>(face3_x(Pm), face3_x(P), ph);
+            __syncthreads();
+            Pm = P;
+            Ur = ur; Uu = uu; Uv = uv; Uw = uw; UE = uE;
+        }
+#pragma unroll 2
+        for (; m < nplanes; ++m) {
+            T ur, uE, uu, uv, uw;
+            load(m, ur, uE, uu, uv, uw);
+            const Flux3<T> fy = yface(m, Pm);
+            const Flux3<T> fz = zface(m);
+            const Cell3<T> P = make_cell3<T, kF>(ur, uu, uv, uw, uE, ph);
+            const Flux3<T> fxhi = face_flux3<T, kF>(face3_x(Pm), face3_x(P), ph);
+            publish_y(m, fy);
+            publish(m, P);
+            __syncthreads();
+            Flux3<T> fzl;
+            fzl.r = __shfl_up_sync(FULL, fz.r, 1);
+            fzl.n = __shfl_up_sync(FULL, fz.n, 1);
+            fzl.t1 = __shfl_up_sync(FULL, fz.t1, 1);
+            fzl.t2 = __shfl_up_sync(FULL, fz.t2, 1);
+            fzl.E = __shfl_up_sync(FULL, fz.E, 1);
+            if (interior) {
+                const auto a0 = S.xF[m & 1][0][t - 32], a1 = S.xF[m & 1][1][t - 32];
+                const Flux3<T> fyl{a0.x, a0.y, a1.x, a1.y, S.xFE[m & 1][t - 32]};
+                const Upd3<T> o = update3<T, kF>(Ur, Uu, Uv, Uw, UE, fxlo, fxhi, fyl, fy, fzl, fz, DtDx, DtDy, DtDz, ph);
+                const long long c = (long long)(g.i0 + m - 2) * g.zy + colofs;
+                rhoE_n[2 * c] = o.r;
+                rhoE_n[2 * c + 1] = o.E;
+                uvw_n[3 * c] = o.u;
+                uvw_n[3 * c + 1] = o.v;
+                uvw_n[3 * c + 2] = o.w;
+                sink(o);
+            }
+            fxlo = fxhi;
+            Pm = P;
+            Ur = ur; Uu = uu; Uv = uv; Uw = uw; UE = uE;
+        }
+    } else if (w == 0) {
+        Cell3<T> Pm0{};
+        for (; m < nplanes; ++m) {
+            T ur, uE, uu, uv, uw;
+            load(m, ur, uE, uu, uv, uw);
+            if (m >= 2) publish_y(m, yface(m, Pm0));
+            const Cell3<T> P0 = make_cell3<T, kF>(ur, uu, uv, uw, uE, ph);
+            publish(m, P0);
+            __syncthreads();
+            Pm0 = P0;
+        }
+    } else {
+        for (; m < nplanes; ++m) {
+            T ur, uE, uu, uv, uw;
+            load(m, ur, uE, uu, uv, uw);
+            publish(m, make_cell3<T, kF>(ur, uu, uv, uw, uE, ph));
+            __syncthreads();
+        }
+    }
+    cp_async_wait<0>();
+    return true;
+}
+
 // One tile march: the lean form for tiles away from walls and ghosts, the general one
 // elsewhere (the choice is uniform over the block). kF: fused arithmetic (hydro_math.cuh).
-// kTma: planes staged by the tensor maps `tm` (march3d_init first); else per-lane copies.
+// kTma: planes staged by the tensor maps `tm` (march3d_init first); else per-lane copies
+// (march3d_lane_roles in strict arithmetic when kLaneRoles, else march3d_lane; the
+// batched engine keeps march3d_lane, where the role split spills in its persistent loop).
 // Returns false when a bounded barrier wait gave up.
-template <class T, bool kF = false, bool kTma = false, int W = k3Warps<T>, class Sink>
+template <class T, bool kF = false, bool kTma = false, int W = k3Warps<T>, bool kLaneRoles = true, class Sink>
 __device__ __forceinline__ bool march3d(Smem3<T, W> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
                                         const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &&sink,
                                         const Tmaps3 &tm = Tmaps3{})
@@ -542,8 +727,13 @@ __device__ __forceinline__ bool march3d(Smem3<T, W> &S, const T *rhoE, const T *
         if (inner) return march3d_tma<false, kF>(S, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, tm, sink);
         return march3d_tma<true, kF>(S, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, tm, sink);
     } else {
-        if (inner) return march3d_lane<false, kF>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
-        return march3d_lane<true, kF>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
+        if constexpr (!kF && kLaneRoles) {
+            if (inner) return march3d_lane_roles<false, kF>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
+            return march3d_lane_roles<true, kF>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
+        } else {
+            if (inner) return march3d_lane<false, kF>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
+            return march3d_lane<true, kF>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
+        }
     }
 }
 
