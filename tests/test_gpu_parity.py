@@ -61,8 +61,10 @@ def test_step2d_bitwise(cuda, oracle, nb, T, kernel):
 @pytest.mark.parametrize("kernel", [hb.KERNEL_STRIP, hb.KERNEL_DIRECT])
 @pytest.mark.parametrize("T", [np.float64, np.float32])
 # (40, 150, 130): 22 x 5 tiles per plane (9-row FP64 tiles; 25 x 5 with 8 rows), most of
-# them interior tiles that take the lean march
-@pytest.mark.parametrize("nb", SHAPES_3D + [(9, 14, 61), (4, 7, 30), (6, 13, 31), (5, 6, 62), (40, 150, 130)])
+# them interior tiles that take the lean march; (3, 8, 34), (2, 1, 64), (5, 15, 30): 9-row
+# tiles whose last tile holds one real row, a single row, a last tile one row short
+@pytest.mark.parametrize("nb", SHAPES_3D + [(9, 14, 61), (4, 7, 30), (6, 13, 31), (5, 6, 62), (40, 150, 130),
+                                            (3, 8, 34), (2, 1, 64), (5, 15, 30)])
 def test_step3d_bitwise(cuda, oracle, nb, T, kernel):
     phys = hb.Physics(T, nb)
     for seed in range(2):
