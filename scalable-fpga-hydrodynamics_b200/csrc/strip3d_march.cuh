@@ -25,12 +25,13 @@
 
 namespace hydro {
 
-// Tile height: 8 warps (6 interior rows) in both precisions. Resident blocks per SM of an
-// 8-warp tile: FP64 two (the 128-register budget; with 16 warps it spills and keeps one
-// block, 31.5 -> 28.4 GCell/s at 512^3), FP32 three (80 registers without spills; 54.1 ->
-// 56.2 GCell/s at 512^3 against two, and 16-warp tiles with one block give 53.7).
-// The plain step also takes other tile heights (warps W per block, W - 2 interior rows),
-// chosen at run time (hydro_set_launch_shape): k3Warps is the default.
+// Warps per block: 8 by default in both precisions (6 interior rows, or 7 in the 9-row
+// tile that the FP64 tensor-map form uses by default). Resident blocks per SM of an 8-warp
+// tile: FP64 two (the 128-register budget; with 16 warps it spills and keeps one block,
+// 31.5 -> 28.4 GCell/s at 512^3 in an earlier form), FP32 three (80 registers without
+// spills; 54.1 -> 56.2 GCell/s at 512^3 against two, and 16-warp tiles with one block give
+// 53.7). The plain step also takes other tile heights, chosen at run time
+// (hydro_set_launch_shape); the batched engine runs k3Warps-row tiles.
 template <class T> constexpr int min_blocks3(int W) { return W <= 8 ? (sizeof(T) == 4 ? 3 : 2) : 1; }
 template <class T> constexpr int k3Warps = 8;                        // y extent of the tile (with halo)
 template <class T> constexpr int k3NT = 32 * k3Warps<T>;             // threads
