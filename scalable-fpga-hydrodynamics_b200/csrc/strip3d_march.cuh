@@ -529,11 +529,12 @@ __device__ __forceinline__ bool march3d_lane(Smem3<T, W> &S, const T *rhoE, cons
     return true;
 }
 
-// Per-lane copies, strict arithmetic: the plane loop written once per warp role, with the
+// Per-lane copies, strict FP64: the plane loop written once per warp role, with the
 // interior rows' +y / +z faces of plane m-1, conversion of plane m and x face in one block
-// ahead of the barrier, as in the tensor-map form (512^3 FP32 56.0 -> 57.2 GCell/s; FP64
-// with an odd NB_Z 31.3 -> 34.0). In fused arithmetic this form measured slower (FP32 63.6 ->
-// 60.4, FP64 35.9 -> 30.7 with spills), so fused keeps march3d_lane.
+// ahead of the barrier, as in the tensor-map form (FP64 with an odd NB_Z, 512 x 512 x 511:
+// 31.3 -> 34.0 GCell/s, no spills against 12 bytes). FP32 keeps march3d_lane: this form
+// ran 56.0 -> 57.2 GCell/s strict at 512^3 but 0.407 -> 0.454 ms at 256^3 (short chunks);
+// in fused arithmetic it measured slower (FP32 63.6 -> 60.4, FP64 35.9 -> 30.7 with spills).
 template <bool kEdge, bool kF, class T, int W, class Sink>
 __device__ __forceinline__ bool march3d_lane_roles(Smem3<T, W> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
                                                const March3 &g, const Phys<T> &ph, T DtDx, T DtDy, T DtDz, Sink &sink)
@@ -715,8 +716,8 @@ __device__ __forceinline__ bool march3d_lane_roles(Smem3<T, W> &S, const T *rhoE
 // One tile march: the lean form for tiles away from walls and ghosts, the general one
 // elsewhere (the choice is uniform over the block). kF: fused arithmetic (hydro_math.cuh).
 // kTma: planes staged by the tensor maps `tm` (march3d_init first); else per-lane copies
-// (march3d_lane_roles in strict arithmetic when kLaneRoles, else march3d_lane; the
-// batched engine keeps march3d_lane, where the role split spills in its persistent loop).
+// (march3d_lane_roles in strict FP64 when kLaneRoles, else march3d_lane; the batched
+// engine keeps march3d_lane, where the role split spills in its persistent loop).
 // Returns false when a bounded barrier wait gave up.
 template <class T, bool kF = false, bool kTma = false, int W = k3Warps<T>, bool kLaneRoles = true, class Sink>
 __device__ __forceinline__ bool march3d(Smem3<T, W> &S, const T *rhoE, const T *uvw, T *rhoE_n, T *uvw_n,
@@ -728,7 +729,7 @@ __device__ __forceinline__ bool march3d(Smem3<T, W> &S, const T *rhoE, const T *
         if (inner) return march3d_tma<false, kF>(S, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, tm, sink);
         return march3d_tma<true, kF>(S, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, tm, sink);
     } else {
-        if constexpr (!kF && kLaneRoles) {
+        if constexpr (!kF && kLaneRoles && sizeof(T) == 8) {
             if (inner) return march3d_lane_roles<false, kF>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
             return march3d_lane_roles<true, kF>(S, rhoE, uvw, rhoE_n, uvw_n, g, ph, DtDx, DtDy, DtDz, sink);
         } else {
