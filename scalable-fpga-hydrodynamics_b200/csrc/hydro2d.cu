@@ -16,11 +16,12 @@
 //  strip2d   one CTA = 128 lanes over 128 consecutive columns (126 interior + one
 //            halo column each side), marching down `chunk` rows. Each row arrives in
 //            shared memory through two TMA tile loads (one per array) into a 4-deep
-//            mbarrier ring; each lane converts its cell to primitives once, computes
-//            the x face above it and the y face to its right once (neighbour inputs and
-//            fluxes exchanged through shared memory with 128-bit accesses), updates the
-//            row above, stores it with 128-bit stores and folds mass, signal speed and
-//            the error checks into the fused epilogue.
+//            mbarrier ring (or per-lane cp.async where TMA rejects the row pitch); each
+//            lane converts its cell to primitives once, computes the x face below it and
+//            the y face to its right once (neighbour inputs and fluxes exchanged through
+//            shared memory with 128-bit accesses), updates the row behind, stores it with
+//            128-bit stores and folds mass, signal speed and the error checks into the
+//            fused epilogue.
 //  direct2d  one thread per cell, scalar loads of the 5-point stencil, every face
 //            evaluated from both sides like the reference. Any alignment, any size;
 //            used when the strip kernel's TMA rules do not hold and as a cross-check.

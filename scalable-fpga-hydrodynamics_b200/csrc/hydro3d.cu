@@ -8,13 +8,15 @@
 // wall cell (hydro3d/kernel.cxx:238-320).
 //
 // Kernels:
-//  strip3d   one CTA = 8 warps over an 8 (y) x 32 (z) tile of columns (6 x 30 interior
-//            plus a one-cell halo ring), marching down `chunk` X planes. Each lane copies
-//            its own cell of each plane into a 4-deep shared-memory ring with cp.async
-//            (any alignment of the interleaved pairs/triples), converts it to primitives
-//            once, and per plane computes one x face (registers), one z face (warp
-//            shuffles) and one y face (shared memory, double-buffered by plane parity,
-//            one barrier per plane), then updates the plane behind it.
+//  strip3d   one CTA of W warps over a tile of rows (y) x 32 (z) columns with a one-cell
+//            halo ring, marching down `chunk` X planes: by default 9 rows on 8 warps
+//            (7 x 30 interior cells; warp 0 holds both halo rows) where tensor maps stage
+//            the planes (FP64, even NB_Z), else 8 rows on 8 warps (6 x 30). Planes arrive
+//            in a shared-memory ring by tensor-map TMA loads or per-lane cp.async (any
+//            alignment of the interleaved pairs/triples); each lane converts its cell to
+//            primitives once and per plane computes one x face (registers), one z face
+//            (flux back by warp shuffles) and one y face (shared memory, double-buffered by
+//            plane parity, one barrier per plane), then updates the plane behind it.
 //  direct3d  one thread per cell, the 7-point stencil loaded directly, every face
 //            evaluated from both sides like the reference.
 #include <algorithm>
