@@ -79,16 +79,18 @@ def test_noalloc_launch_shape_fits_the_fixed_scratch(built):
 
 
 def test_launch_shape_settings(built):
-    """hydro_set_launch_shape (host only): the tile heights the 3D kernels are built for and
-    the 2D register budgets are accepted, anything else rejected with HYDRO_ERR_ARG; 0
-    restores the built-in shape."""
+    """hydro_set_launch_shape (host only): the tile heights the 3D kernels are built for (in
+    rows with the halo: 8, 16, and in FP64 also 9 and 12) and the 2D register budgets are
+    accepted, anything else rejected with HYDRO_ERR_ARG; 0 restores the built-in shape."""
     fn = built.hydro_set_launch_shape
     fn.argtypes = [ctypes.c_int] * 5
     fn.restype = ctypes.c_int
-    for args in ((3, 8, 8, 0, 0), (3, 8, 12, 64, 0), (3, 8, 16, 32, 0), (3, 4, 8, 0, 0), (3, 4, 16, 128, 0),
+    for args in ((3, 8, 8, 0, 0), (3, 8, 9, 0, 0), (3, 8, 9, 128, 0), (3, 8, 12, 64, 0), (3, 8, 16, 32, 0),
+                 (3, 4, 8, 0, 0), (3, 4, 16, 128, 0),
                  (2, 8, 0, 64, 0), (2, 4, 0, 0, 0), (2, 8, 0, 0, 5), (2, 4, 0, 32, 8), (2, 8, 0, 0, 4)):
         assert fn(*args) == 0, args
-    for args in ((3, 4, 12, 0, 0), (3, 8, 10, 0, 0), (2, 8, 8, 0, 0), (4, 8, 0, 0, 0), (3, 2, 8, 0, 0),
+    for args in ((3, 4, 12, 0, 0), (3, 4, 9, 0, 0), (3, 8, 10, 0, 0), (3, 8, 7, 0, 0), (2, 8, 9, 0, 0),
+                 (2, 8, 8, 0, 0), (4, 8, 0, 0, 0), (3, 2, 8, 0, 0),
                  (3, 8, 8, -1, 0), (2, 8, 0, 0, 8), (2, 4, 0, 0, 5), (3, 8, 8, 0, 4)):
         assert fn(*args) == hb.HYDRO_ERR_ARG, args
     for dim in (2, 3):
